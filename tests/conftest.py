@@ -1,0 +1,18 @@
+import os
+import sys
+
+import pytest
+
+REPO = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+if REPO not in sys.path:
+    sys.path.insert(0, REPO)
+
+
+def pytest_configure(config):
+    config.addinivalue_line("markers", "gpu: needs a CUDA device (B200); runs the CUDA path")
+
+
+@pytest.fixture(scope="session")
+def kat():
+    import numpy as np
+    return np.load(os.path.join(REPO, "tests", "golden", "kat_cases.npz"))
