@@ -1,0 +1,82 @@
+// context.h -- the FftContext behind the opaque handle of libfft_cffi.so.
+//
+// Mirrors the fields of the reference context (fft_cffi.cpp:40-82) and adds
+// the device state that replaces the reference's PlanCache + WorkerPool: one
+// CUDA stream, device-resident windows and grow-only staging buffers.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <mutex>
+#include <vector>
+
+#include "kernels.h"
+
+namespace ffb {
+
+// Grow-only device buffer.
+struct DevBuf {
+  void* p = nullptr;
+  size_t cap = 0;
+  void* get(size_t bytes);
+  void release();
+  ~DevBuf() { release(); }
+};
+
+struct FftContext {
+  uint32_t magic = 0x46465442u;  // "FFTB"
+  // --- reference fields ---
+  int N = 0;
+  bool inverse = false;
+  int kernel = 0;  // 0 = auto (Cooley-Tukey), 1 = Cooley-Tukey, 2 = Stockham
+  int radix = 0;
+  int pad_mode = 0;
+  std::vector<int> radix_pattern;
+  int window = 0;
+  int hop = 0;
+  int transform = 0;
+  int reduce_magnitude = 0;
+  int store_polar = 0;
+  int half_spectrum = 0;
+  int allow_outer_parallel = 1;
+  int allow_inner_parallel = 0;
+  int inner_threads = 0;
+  int threads = 1;  // PlanRuntimeConfig::threads as the reference stores it
+  int lanes = 1;
+  bool has_pool = false;  // the reference creates a WorkerPool here
+  int analysis_win_kind = 0, synthesis_win_kind = 0;
+  float win_param1 = 0.f, win_param2 = 0.f;
+  int win_norm_policy = 0, cola_mode = 0;
+  std::vector<float> analysis_win, synthesis_win;
+  bool windows_enabled = false;
+  int apply_ola = 0;
+  // streaming state (fft_cffi.cpp:72-78)
+  std::vector<float> streaming_buffer;
+  size_t streaming_offset = 0;
+  std::vector<float> streaming_inverse_queue;
+  size_t streaming_inverse_offset = 0;
+  std::vector<float> streaming_inverse_accum;
+  std::vector<float> streaming_inverse_norm;
+
+  // --- device state ---
+  int device = 0;
+  cudaStream_t own_stream = nullptr;
+  cudaStream_t stream = nullptr;
+  bool async = false;
+  int logr_req = -1;  // requested pass radix (log2), -1 = autotuned default
+  DevBuf d_analysis, d_synthesis, d_weight;
+  bool windows_uploaded = false;
+  DevBuf d_in0, d_in1, d_out0, d_out1, d_out2, d_frames;
+  uint64_t launches = 0;
+  std::recursive_mutex mu;
+
+  int eff_transform() const { return (transform >= 0 && transform <= 3) ? transform : 0; }
+  bool stockham() const { return kernel == 2; }
+  int bins() const { return half_spectrum ? N / 2 + 1 : N; }
+  PostFlags post_flags() const;
+};
+
+FftContext* as_ctx(void* h);
+
+}  // namespace ffb

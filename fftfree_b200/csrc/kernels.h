@@ -1,0 +1,89 @@
+// kernels.h -- host-side launchers of the sm_100a kernels (C++ linkage,
+// internal to libfft_cffi.so).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stddef.h>
+#include <stdint.h>
+
+namespace ffb {
+
+// Post-transform hook flags (reference eigen_fft.hpp:2535-2596).
+struct PostFlags {
+  int r2c_half;    // R2C && half_spectrum: DC/Nyquist imag <- 0, bins > N/2 <- 0
+  int polar;       // store_polar: (|v|, arg v)
+  int reduce;      // reduce_magnitude: (|v|, 0)
+  int clear_imag;  // C2R without polar/reduce: imag <- 0
+};
+
+// Real frames -> spectrum (fft_execute_batched, fft_execute, fft_pcm_to_channels).
+struct StftArgs {
+  const float* pcm;
+  long long pcm_len;
+  long long frames;
+  int N, W, H;
+  const float* win;  // device, length >= W, or nullptr
+  int mirror;        // Cooley-Tukey + C2R + half: x[n] = x[N-n] for n > N/2
+  int inverse;
+  PostFlags pf;
+  int out_bins;
+  long long out_stride;
+  int mag_from_real;  // out_mag = re when store_polar (fft_cffi.cpp:822)
+  float* out_re;
+  float* out_im;
+  float* out_mag;
+};
+
+// Complex columns in/out with the plan hooks (C++ fft_inplace_batched).
+struct C2cArgs {
+  const float2* in;
+  float2* out;
+  long long batch;
+  int N;
+  int pre;       // 0 none, 1 R2C imag clear, 2 C2R half mirror (+polar)
+  int polar_in;  // polar conversion in pre == 2
+  int inverse;
+  PostFlags pf;
+};
+
+// Planar complex frames -> real frames (fft_execute_complex_batched).
+struct CplxBatchArgs {
+  const float* in_re;
+  const float* in_im;
+  long long frames;
+  int N, bins;
+  int c2r_half;  // Hermitian rebuild of fft_cffi.cpp:1072-1093
+  int ct_pre;    // Cooley-Tukey pre-hook: 0 none, 1 R2C imag clear, 2 C2R half
+  int polar_in;
+  int inverse;
+  PostFlags pf;
+  const float* synth;  // device window or nullptr
+  float* out;          // frames x N
+};
+
+struct OlaArgs {
+  const float* frames_buf;  // frames x N
+  long long frames;
+  int N, H;
+  int cola;
+  const float* weight;  // device, N entries (analysis*synthesis) or nullptr (=1)
+  float* out;           // frames * N samples
+};
+
+// Twiddle pyramid (levels 0..max_log) on the current device.
+const float2* twiddle_pyramid(int max_log, cudaStream_t stream);
+
+// Pick the single-pass radix (log2) for a transform of 2^logm points;
+// `requested_log` (2..4) is honoured when valid.  Returns -1 if the size
+// needs the multi-pass path.
+int choose_logr(int logm, int requested_log);
+int max_single_pass_log();
+
+// Launchers return cudaSuccess or the launch error.  `launches` is
+// incremented by the number of kernels enqueued.
+cudaError_t launch_stft(const StftArgs& a, int logr, cudaStream_t s, uint64_t* launches);
+cudaError_t launch_c2c(const C2cArgs& a, int logr, cudaStream_t s, uint64_t* launches);
+cudaError_t launch_cplx_batch(const CplxBatchArgs& a, int logr, cudaStream_t s, uint64_t* launches);
+cudaError_t launch_ola(const OlaArgs& a, cudaStream_t s, uint64_t* launches);
+
+}  // namespace ffb

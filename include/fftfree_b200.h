@@ -1,0 +1,77 @@
+/*
+ * fftfree_b200.h -- additive extensions of libfft_cffi.so (B200 build).
+ *
+ * These entry points have no C-ABI counterpart in the reference; each one
+ * names the reference C++ API it exposes.  All keep the reference
+ * conventions: plain pointers and sizes, 0 on failure, no exceptions.
+ */
+#ifndef FFTFREE_B200_EXT_H
+#define FFTFREE_B200_EXT_H
+
+#include <stddef.h>
+#include "fft_cffi.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Complex-in / complex-out batched transform with the context's plan flags
+ * (transform mode, hooks, inverse, kernel) -- the reference C++ API
+ * eigfft::fft_inplace_batched (eigen_fft.hpp:3170-3175), which the reference
+ * C ABI does not expose (its complex entry returns only the real part).
+ * `in` and `out` hold `batch` transforms of N interleaved complex floats
+ * each (the N x batch column-major matrix of the C++ API); they may alias.
+ * Returns 1 on success. */
+FFT_CFFI_API int fftfree_execute_c2c(void* handle, const float* in, float* out, size_t batch);
+
+/* One metadata request: the fields of eigfft::MetadataRequest
+ * (eigen_fft.hpp:1496-1501); `buffer` holds `count` interleaved complex
+ * floats.  Kinds are eigfft::MetadataKind ordinals (eigen_fft.hpp:1477-1491):
+ * 0 Twiddle, 1 LayoutMap, 2 StageSnapshot, 3 StageParams, 4 ButterflyPairs,
+ * 5 StageInvariant, 6 TwiddleIndexMap, 7 Omega, 8 StageSnapshotAll,
+ * 9 ButterflyPairsAll, 10 TwiddleIndexMapAll. */
+typedef struct fftfree_metadata_request {
+  int kind;
+  float* buffer;
+  size_t count;
+} fftfree_metadata_request;
+
+/* eigfft::fft_inplace_batched_with_metadata (eigen_fft.hpp:3152-3168): the
+ * transform of fftfree_execute_c2c executed as the literal radix-2 stage
+ * sequence of the context's kernel (Cooley-Tukey or Stockham), filling the
+ * requested metadata.  Returns 0 when a buffer is too small (the reference
+ * throws std::invalid_argument there). */
+FFT_CFFI_API int fftfree_execute_c2c_meta(void* handle, const float* in, float* out, size_t batch,
+                                          const fftfree_metadata_request* requests,
+                                          int request_count);
+
+/* Run the context's work on this CUDA stream (a cudaStream_t); NULL restores
+ * the context's own stream. */
+FFT_CFFI_API void fftfree_set_stream(void* handle, void* cuda_stream);
+
+/* When on, a call whose buffers are all device memory returns once its work
+ * is enqueued on the context stream instead of waiting for it. */
+FFT_CFFI_API void fftfree_set_async(void* handle, int on);
+
+/* Number of kernels this context has launched so far. */
+FFT_CFFI_API unsigned long long fftfree_ctx_launch_count(void* handle);
+
+/* Radix schedule (per pass) that the context's plan executes for its main
+ * transform; returns the number of passes written (at most max_passes). */
+FFT_CFFI_API int fftfree_ctx_schedule(void* handle, int* radices, int max_passes);
+
+/* 1 when a CUDA device is usable by this library, else 0. */
+FFT_CFFI_API int fftfree_device_available(void);
+
+/* Test hook of the recovery coordinator (fft_cffi.cpp:954-982): runs the
+ * host-side dropout / restore / split decisions for one batch of `frames`
+ * frames, invoking the registered restore observer as the recovery path
+ * would, and writes 1 into raw_out[f] for each frame left in its restored
+ * (untransformed) state.  Needs no GPU.  Returns the number of such frames. */
+FFT_CFFI_API size_t fftfree_debug_recovery_plan(size_t frames, char* raw_out);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif

@@ -182,15 +182,19 @@ static int collect_meta(const oracle_cfg* c, size_t B, const oracle_meta_req* re
     const int k = reqs[i].kind;
     cf* buf = (cf*)reqs[i].buf;
     const size_t cnt = reqs[i].count;
-    if (k < 0 || k > 10 || seen[k]) continue; /* first request of a kind wins */
+    if (k < 0 || k > 10) continue;
+    if (k == ORACLE_META_TWIDDLE) {
+      /* eigen_fft.hpp:1538-1558: every Twiddle request is validated and the
+       * last one is the buffer written (the loop has no break). */
+      size_t total = 0;
+      for (int s = 0; s < S; ++s) total += (size_t)1 << s;
+      if (total > 0 && (!buf || cnt < total)) return 0;
+      m->twiddle = buf; m->twiddle_n = total;
+      continue;
+    }
+    if (seen[k]) continue; /* the other writers stop at the first request */
     seen[k] = 1;
     switch (k) {
-      case ORACLE_META_TWIDDLE: { /* eigen_fft.hpp:1538-1558 */
-        size_t total = 0;
-        for (int s = 0; s < S; ++s) total += (size_t)1 << s;
-        if (total > 0 && (!buf || cnt < total)) return 0;
-        m->twiddle = buf; m->twiddle_n = total; break;
-      }
       case ORACLE_META_LAYOUT_MAP: /* :1604-1619 */
         if (buf && cnt < (size_t)N) return 0;
         m->layout = buf; break;
@@ -214,9 +218,10 @@ static int collect_meta(const oracle_cfg* c, size_t B, const oracle_meta_req* re
         if (S <= 0) break;
         if (!buf || cnt < NS) return 0;
         m->twmap = buf; break;
-      case ORACLE_META_OMEGA: /* :1772-1786; Cooley-Tukey only */
+      case ORACLE_META_OMEGA: /* :1772-1786; constructed by Cooley-Tukey only */
+        if (stockham) break;
         if (buf && cnt < (size_t)N) return 0;
-        if (!stockham) m->omega = buf;
+        m->omega = buf;
         break;
       case ORACLE_META_STAGE_SNAPSHOT_ALL:
       case ORACLE_META_BUTTERFLY_PAIRS_ALL:
