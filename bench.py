@@ -1,0 +1,366 @@
+"""Benchmark of the batched FFT hot path on B200 (one JSON line on stdout).
+
+Workload (N=1 line): batched C2C forward, N = 4096 points x 16,384 transforms,
+complex64, inputs re/im i.i.d. N(0,1) from seed 1, Stockham order -- the
+batched-C2C configuration of the reference (fft_inplace_batched over a
+4096 x 16384 column-major matrix).  One step = one pass over the whole batch.
+
+  value  -- device-resident throughput: algorithmic bytes (input read once +
+            output written once, 1 GiB per pass) / device time, all ranks.
+  e2e    -- the same transform through the public C ABI with pinned HOST
+            buffers: H2D of the input, kernel, D2H of the output, per step.
+  roofline -- the FFT kernel alone, timed with CUDA events on its stream,
+            against the measured HBM copy bandwidth.
+  cpu_baseline -- the CPU oracle (a port of the reference executor) on the
+            host cores, on a bounded sample of the same transforms.
+
+--impl reference times that CPU port alone (the reference itself needs
+Eigen, which is not installed, so its C++ cannot be built here).
+Multi-GPU (torchrun): every rank runs its own batch (weak scaling, no
+data-path collective); time is the max over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+REPO = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, REPO)
+
+METRIC = "STFT GB/s (% HBM peak); autograd fwd+bwd vs plain fwd at rel-L2<=1e-5 vs FP64"
+N_FFT = 4096
+BATCH = 16384
+BYTES_PER_PASS = 2 * N_FFT * BATCH * 8  # read + write, complex64
+
+
+def _peaks():
+    try:
+        with open(os.path.join(REPO, "MEASURED_PEAKS.json")) as f:
+            p = json.load(f)
+        return float(p["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def _profile_traffic():
+    """DRAM bytes per launch of the C2C kernel from the committed ncu summary."""
+    try:
+        with open(os.path.join(REPO, "profiles", "c2c_n4096_traffic.json")) as f:
+            return json.load(f).get("dram_bytes_per_launch")
+    except Exception:
+        return None
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    def __init__(self, index: int):
+        self.index = index
+        self.samples = []
+        self._stop = threading.Event()
+        self._t = None
+
+    def _run(self):
+        q = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+             "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+             "clocks_event_reasons.sw_power_cap")
+        while not self._stop.is_set():
+            try:
+                out = subprocess.run(["nvidia-smi", "-i", str(self.index), f"--query-gpu={q}",
+                                      "--format=csv,noheader,nounits"], capture_output=True, text=True,
+                                     timeout=5).stdout.strip()
+                if out:
+                    self.samples.append([x.strip() for x in out.split(",")])
+            except Exception:
+                pass
+            self._stop.wait(0.2)
+
+    def __enter__(self):
+        self._t = threading.Thread(target=self._run, daemon=True)
+        self._t.start()
+        return self
+
+    def __exit__(self, *a):
+        self._stop.set()
+        if self._t:
+            self._t.join(timeout=10)
+
+    def summary(self):
+        if not self.samples:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(s[0]) for s in self.samples if s[0].replace(".", "").isdigit()]
+        mx = [float(s[1]) for s in self.samples if s[1].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for s in self.samples for i in range(4) if len(s) > 3 + i and
+                          s[3 + i].lower().startswith("active")})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(self.samples)}
+
+
+def cpu_baseline(threads: int, budget_s: float = 12.0):
+    """The CPU port of the reference executor on a bounded sample."""
+    import numpy as np
+    from oracle.oracle import OracleContext
+    rng = np.random.default_rng(1)
+    B = 1024
+    x = (rng.standard_normal((B, N_FFT)) + 1j * rng.standard_normal((B, N_FFT))).astype(np.complex64)
+    ctx = OracleContext(N=N_FFT, kernel=2)
+    ctx.fft_columns(x[:64], threads=threads)  # warm-up
+    times = []
+    t_end = time.perf_counter() + budget_s
+    while time.perf_counter() < t_end or len(times) < 3:
+        t0 = time.perf_counter()
+        ctx.fft_columns(x, threads=threads)
+        times.append(time.perf_counter() - t0)
+        if len(times) >= 50:
+            break
+    t = statistics.median(times)
+    gbs = 2 * B * N_FFT * 8 / t / 1e9
+    return {"value": round(gbs, 3), "unit": "GB/s", "cores": threads, "kind": "port",
+            "sample": f"{B} of {BATCH} transforms (N={N_FFT} C2C forward, Stockham order) per rep, "
+                      f"median of {len(times)} reps, {threads} OpenMP threads"}
+
+
+def run_reference(args, rank, world):
+    if rank != 0:
+        return 0
+    threads = os.cpu_count() or 1
+    import numpy as np
+    from oracle.oracle import OracleContext
+    rng = np.random.default_rng(1)
+    B = 1024
+    x = (rng.standard_normal((B, N_FFT)) + 1j * rng.standard_normal((B, N_FFT))).astype(np.complex64)
+    ctx = OracleContext(N=N_FFT, kernel=2)
+    for _ in range(args.warmup):
+        ctx.fft_columns(x, threads=threads)
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        ctx.fft_columns(x, threads=threads)
+    dt = (time.perf_counter() - t0) / args.steps
+    value = 2 * B * N_FFT * 8 / dt / 1e9
+    line = {"impl": "reference", "metric": METRIC, "value": round(value, 3), "unit": "GB/s", "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(dt * 1e3, 3),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "c64",
+            "data": "synthetic",
+            "config": {"workload": f"batched C2C forward N={N_FFT}, bounded sample of {B} of {BATCH} transforms "
+                                   f"per step (host CPU port of the reference radix-2 Stockham executor)",
+                       "parallelism": "host threads"},
+            "cpu_baseline": {"value": round(value, 3), "unit": "GB/s", "cores": threads, "kind": "port",
+                             "sample": f"{B} transforms of N={N_FFT} per step"},
+            "e2e": {"value": round(value, 3), "unit": "GB/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-legs", action="store_true")
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        return run_reference(args, rank, world)
+
+    import numpy as np
+    import torch
+    import fftfree_b200 as ff
+
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", local))
+
+    peak, peak_kind = _peaks()
+    stream = torch.cuda.Stream()
+    torch.cuda.set_stream(stream)
+    g = torch.Generator(device="cuda").manual_seed(1 + rank)
+    x = torch.randn(BATCH, N_FFT, 2, device="cuda", generator=g)
+    y = torch.empty_like(x)
+    ctx = ff.FftContext.full_v2(N_FFT, kernel=2)
+    ctx.set_stream(stream.cuda_stream)
+    ctx.set_async(True)
+
+    def step():
+        if ctx.execute_c2c(x, y, BATCH) != 1:
+            raise RuntimeError("fftfree_execute_c2c failed")
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    launches0 = ctx.launch_count()
+    evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    with ClockSampler(local) as clocks:
+        torch.cuda.synchronize()
+        t_start = torch.cuda.Event(enable_timing=True)
+        t_stop = torch.cuda.Event(enable_timing=True)
+        t_start.record(stream)
+        for i in range(args.steps):
+            evs[i][0].record(stream)
+            step()
+            evs[i][1].record(stream)
+        t_stop.record(stream)
+        torch.cuda.synchronize()
+    launches = ctx.launch_count() - launches0
+    total_ms = t_start.elapsed_time(t_stop)
+    kern_ms = [a.elapsed_time(b) for a, b in evs]
+    if dist:
+        t = torch.tensor([total_ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        total_ms = float(t.item())
+        dist.barrier()
+    ms_per_step = total_ms / args.steps
+    value = BYTES_PER_PASS * world * args.steps / (total_ms * 1e-3) / 1e9
+    kern_avg = sum(kern_ms) / len(kern_ms)
+    achieved = BYTES_PER_PASS / (kern_avg * 1e-3) / 1e9
+
+    # secondary legs on the same device (information; not the headline)
+    legs = {}
+    if rank == 0 and not args.no_legs:
+        legs = measure_legs(ff, torch, stream)
+
+    # e2e through the C ABI with pinned host buffers
+    e2e = None
+    if not args.no_e2e:
+        hx = torch.empty(BATCH, N_FFT, 2, pin_memory=True)
+        hx.copy_(x.cpu())
+        hy = torch.empty_like(hx).pin_memory()
+        ctx_h = ff.FftContext.full_v2(N_FFT, kernel=2)
+        for _ in range(2):
+            ctx_h.execute_c2c(hx, hy, BATCH)
+        n_e2e = max(3, min(args.steps, 10))
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for _ in range(n_e2e):
+            if ctx_h.execute_c2c(hx, hy, BATCH) != 1:
+                raise RuntimeError("e2e call failed")
+        dt = (time.perf_counter() - t0) / n_e2e
+        e2e_val = BYTES_PER_PASS / dt / 1e9
+        if dist:
+            t = torch.tensor([dt], device="cuda")
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            e2e_val = BYTES_PER_PASS * world / float(t.item()) / 1e9
+        e2e = {"value": round(e2e_val, 3), "unit": "GB/s", "h2d_bytes_per_step": BATCH * N_FFT * 8,
+               "d2h_bytes_per_step": BATCH * N_FFT * 8, "ms_per_step": round(dt * 1e3, 3)}
+        ctx_h.close()
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cpu = cpu_baseline(os.cpu_count() or 1)
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": round(value, 3), "unit": "GB/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": round(ms_per_step, 4), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "c64", "data": "synthetic",
+            "config": {"workload": f"batched C2C forward, N={N_FFT} x {BATCH} transforms complex64 per GPU "
+                                   f"(Stockham order), N(0,1) re/im, device-resident",
+                       "l2": "inputs larger than L2 (512 MiB in, 512 MiB out per pass)",
+                       "parallelism": f"replicas x{world}" if world > 1 else "single GPU"},
+            "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+                         "frac": round(achieved / peak, 4), "traffic": _profile_traffic(),
+                         "peak_kind": f"{peak_kind} (hbm_gbs)", "kernel": "k_fft<Sched<12,4>,C2cIO>",
+                         "kernel_ms": round(kern_avg, 4)},
+            "e2e": e2e,
+            "gpu_launches": launches,
+            "clocks": clocks.summary(),
+            "legs": legs,
+        }
+        if cpu:
+            line["cpu_baseline"] = cpu
+        print(json.dumps(line), flush=True)
+    ctx.close()
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+def measure_legs(ff, torch, stream, reps: int = 10):
+    """Other legs of the configuration, device-resident, CUDA-event timed."""
+    import numpy as np
+
+    def timed(fn, nbytes):
+        for _ in range(3):
+            fn()
+        torch.cuda.synchronize()
+        a = torch.cuda.Event(enable_timing=True)
+        b = torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        for _ in range(reps):
+            fn()
+        b.record(stream)
+        torch.cuda.synchronize()
+        ms = a.elapsed_time(b) / reps
+        return {"ms": round(ms, 4), "GB/s": round(nbytes / (ms * 1e-3) / 1e9, 1)}
+
+    legs = {}
+    g = torch.Generator(device="cuda").manual_seed(1)
+    x = torch.randn(BATCH, N_FFT, 2, device="cuda", generator=g)
+    y = torch.empty_like(x)
+    for name, kw in [("c2c_inverse_stockham", dict(kernel=2, inverse=1)),
+                     ("c2c_forward_cooleytukey", dict(kernel=1)),
+                     ("c2c_inverse_cooleytukey", dict(kernel=1, inverse=1))]:
+        c = ff.FftContext.full_v2(N_FFT, **kw)
+        c.set_stream(stream.cuda_stream)
+        c.set_async(True)
+        legs[name] = timed(lambda: c.execute_c2c(x, y, BATCH), BYTES_PER_PASS)
+        c.close()
+    # R2C via fft_execute_batched, W = H = N = 4096, half spectrum, polar
+    pcm = torch.rand(BATCH * N_FFT, device="cuda", generator=g) * 2 - 1
+    bins = N_FFT // 2 + 1
+    re = torch.empty(BATCH * bins, device="cuda"); im = torch.empty_like(re); mag = torch.empty_like(re)
+    c = ff.FftContext.full_v2(N_FFT, kernel=2, window=N_FFT, hop=N_FFT, transform=1, half_spectrum=1, store_polar=1)
+    c.set_stream(stream.cuda_stream)
+    c.set_async(True)
+    legs["r2c_stft_n4096_half_polar"] = timed(
+        lambda: c.execute_batched(pcm, re, im, mag, pcm_len=BATCH * N_FFT),
+        BATCH * N_FFT * 4 + 3 * BATCH * bins * 4)
+    c.close()
+    # C2R round trip leg: half spectrum, polar input, inverse
+    out = torch.empty(BATCH * N_FFT, device="cuda")
+    c = ff.FftContext.full_v2(N_FFT, kernel=0, inverse=1, transform=2, half_spectrum=1, store_polar=1)
+    c.set_stream(stream.cuda_stream)
+    c.set_async(True)
+    legs["c2r_n4096_half_polar"] = timed(lambda: c.execute_complex_batched(re, im, BATCH, out),
+                                         2 * BATCH * bins * 4 + BATCH * N_FFT * 4)
+    c.close()
+    # config-1 shape on a long signal: N=W=1024, H=256, half, magnitude
+    L = 512 * 65536
+    pcm1 = torch.rand(L, device="cuda", generator=g) * 2 - 1
+    frames = 1 + (L - 1024) // 256
+    b1 = 513
+    re1 = torch.empty(frames * b1, device="cuda"); im1 = torch.empty_like(re1); mag1 = torch.empty_like(re1)
+    c = ff.FftContext.full_v2(1024, kernel=2, radix=4, window=1024, hop=256, transform=1, reduce_magnitude=1,
+                              half_spectrum=1)
+    c.set_stream(stream.cuda_stream)
+    c.set_async(True)
+    legs["stft_r2c_n1024_h256_long_signal"] = timed(
+        lambda: c.execute_batched(pcm1, re1, im1, mag1, pcm_len=L), L * 4 + 3 * frames * b1 * 4)
+    legs["stft_r2c_n1024_h256_long_signal"]["frames_per_s"] = round(
+        frames / (legs["stft_r2c_n1024_h256_long_signal"]["ms"] * 1e-3), 1)
+    c.close()
+    return legs
+
+
+if __name__ == "__main__":
+    sys.exit(main())

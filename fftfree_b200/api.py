@@ -92,6 +92,7 @@ _SIGS = [
     ("fftfree_execute_c2c_meta", ctypes.c_int, [ctypes.c_void_p, c_float_p, c_float_p, ctypes.c_size_t,
                                                 ctypes.POINTER(MetadataRequest), ctypes.c_int]),
     ("fftfree_set_stream", None, [ctypes.c_void_p, ctypes.c_void_p]),
+    ("fftfree_ctx_stream", ctypes.c_void_p, [ctypes.c_void_p]),
     ("fftfree_set_async", None, [ctypes.c_void_p, ctypes.c_int]),
     ("fftfree_ctx_launch_count", ctypes.c_ulonglong, [ctypes.c_void_p]),
     ("fftfree_ctx_schedule", ctypes.c_int, [ctypes.c_void_p, c_int_p, ctypes.c_int]),
@@ -206,7 +207,12 @@ class FftContext:
         return int(lib().fftfree_ctx_launch_count(self.handle))
 
     def set_stream(self, stream_handle: Optional[int]):
+        """Run on this cudaStream_t (an int handle, e.g. torch's
+        ``stream.cuda_stream``; 0 is the legacy default stream)."""
         lib().fftfree_set_stream(self.handle, ctypes.c_void_p(stream_handle or 0))
+
+    def stream(self) -> int:
+        return int(lib().fftfree_ctx_stream(self.handle) or 0)
 
     def set_async(self, on: bool):
         lib().fftfree_set_async(self.handle, 1 if on else 0)
@@ -236,7 +242,10 @@ class FftContext:
         for i, (kind, buf) in enumerate(requests):
             arr[i].kind = kind
             arr[i].buffer = _fp(buf.view(np.float32)) if isinstance(buf, np.ndarray) else _fp(buf)
-            arr[i].count = buf.size if isinstance(buf, np.ndarray) else buf.numel()
+            if isinstance(buf, np.ndarray):
+                arr[i].count = buf.size if np.iscomplexobj(buf) else buf.size // 2
+            else:  # torch tensor: complex dtype, or interleaved floats
+                arr[i].count = buf.numel() if buf.is_complex() else buf.numel() // 2
         return int(lib().fftfree_execute_c2c_meta(self.handle, _fp(x), _fp(out), batch, arr, len(requests)))
 
 

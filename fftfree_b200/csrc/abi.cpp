@@ -32,6 +32,9 @@
 
 namespace ffb {
 
+int run_meta(FftContext* c, const float* in, float* out, size_t batch, const fftfree_metadata_request* reqs,
+             int nreq);
+
 // ------------------------------------------------------------------ utilities
 static bool verbose() {
   static const bool v = [] {
@@ -627,6 +630,7 @@ FFT_CFFI_API void fft_free(void* handle) {
     c->d_out1.release();
     c->d_out2.release();
     c->d_frames.release();
+    c->d_meta_tw.release();
     c->magic = 0;
   }
   delete c;
@@ -893,11 +897,30 @@ FFT_CFFI_API int fftfree_execute_c2c(void* handle, const float* in, float* out, 
   }
 }
 
+FFT_CFFI_API int fftfree_execute_c2c_meta(void* handle, const float* in, float* out, size_t batch,
+                                          const fftfree_metadata_request* requests, int request_count) {
+  FftContext* c = as_ctx(handle);
+  if (!c || !in || !out || batch == 0) return 0;
+  if (request_count > 0 && !requests) return 0;
+  try {
+    std::lock_guard<std::recursive_mutex> lk(c->mu);
+    DeviceGuard g(c->device);
+    return run_meta(c, in, out, batch, requests, request_count);
+  } catch (...) {
+    return 0;
+  }
+}
+
 FFT_CFFI_API void fftfree_set_stream(void* handle, void* cuda_stream) {
   FftContext* c = as_ctx(handle);
   if (!c) return;
   std::lock_guard<std::recursive_mutex> lk(c->mu);
-  c->stream = cuda_stream ? static_cast<cudaStream_t>(cuda_stream) : c->own_stream;
+  c->stream = static_cast<cudaStream_t>(cuda_stream);
+}
+
+FFT_CFFI_API void* fftfree_ctx_stream(void* handle) {
+  FftContext* c = as_ctx(handle);
+  return c ? static_cast<void*>(c->stream) : nullptr;
 }
 
 FFT_CFFI_API void fftfree_set_async(void* handle, int on) {

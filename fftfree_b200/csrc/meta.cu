@@ -349,8 +349,7 @@ int run_meta(FftContext* c, const float* in, float* out, size_t batch, const fft
   }
   float2* A = static_cast<float2*>(c->d_frames.get(n * sizeof(float2)));
   float2* Bf = stockham ? static_cast<float2*>(c->d_out1.get(n * sizeof(float2))) : nullptr;
-  float2* d_W = static_cast<float2*>(c->d_weight.get(W.size() * sizeof(float2)));
-  c->windows_uploaded = false;  // d_weight is reused here; windows upload again on demand
+  float2* d_W = static_cast<float2*>(c->d_meta_tw.get(W.size() * sizeof(float2)));
   ck(cudaMemcpyAsync(d_W, W.data(), W.size() * sizeof(float2), cudaMemcpyHostToDevice, st));
   auto dev_target = [&](Req& r, DevBuf& tmp) -> float2* {
     if (!r.user) return nullptr;

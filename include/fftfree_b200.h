@@ -45,9 +45,14 @@ FFT_CFFI_API int fftfree_execute_c2c_meta(void* handle, const float* in, float* 
                                           const fftfree_metadata_request* requests,
                                           int request_count);
 
-/* Run the context's work on this CUDA stream (a cudaStream_t); NULL restores
- * the context's own stream. */
+/* Run the context's work on this CUDA stream (a cudaStream_t, used as given:
+ * NULL is CUDA's legacy default stream).  A context starts on a non-blocking
+ * stream of its own; fftfree_ctx_stream() returns the current one, so a
+ * caller can put it back later. */
 FFT_CFFI_API void fftfree_set_stream(void* handle, void* cuda_stream);
+
+/* The CUDA stream the context currently runs on. */
+FFT_CFFI_API void* fftfree_ctx_stream(void* handle);
 
 /* When on, a call whose buffers are all device memory returns once its work
  * is enqueued on the context stream instead of waiting for it. */
