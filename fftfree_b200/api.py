@@ -97,6 +97,8 @@ _SIGS = [
     ("fftfree_ctx_launch_count", ctypes.c_ulonglong, [ctypes.c_void_p]),
     ("fftfree_ctx_schedule", ctypes.c_int, [ctypes.c_void_p, c_int_p, ctypes.c_int]),
     ("fftfree_device_available", ctypes.c_int, []),
+    ("fftfree_execute_complex_batched_noalloc", ctypes.c_size_t, [ctypes.c_void_p, c_float_p, c_float_p,
+                                                                   ctypes.c_size_t, c_float_p, ctypes.c_size_t]),
     ("fftfree_debug_recovery_plan", ctypes.c_size_t, [ctypes.c_size_t, ctypes.c_char_p]),
 ]
 

@@ -68,6 +68,25 @@ FFT_CFFI_API int fftfree_ctx_schedule(void* handle, int* radices, int max_passes
 /* 1 when a CUDA device is usable by this library, else 0. */
 FFT_CFFI_API int fftfree_device_available(void);
 
+/* No counterpart in the reference.  fft_execute_complex_batched (fast path,
+ * with the context's windows and overlap-add) for callers that cannot
+ * allocate GPU memory while they run -- a real-time audio thread, for which
+ * cudaMalloc / cudaFree may block and synchronise the device, or a process
+ * whose GPU memory is all reserved up front by another allocator.  The call
+ * allocates nothing: all three buffers must be device memory (host buffers
+ * are rejected, they would need staging), and the per-frame samples that the
+ * overlap-add sums are kept in a fixed 16 MiB array compiled into the
+ * library, which every GPU that loads the library holds until exit.  Limit:
+ * frames * N <= 4,194,304 when the context applies overlap-add; larger calls
+ * are rejected with a message on stderr and return 0.  The first call on a
+ * device looks up that array's device address (cudaGetSymbolAddress) and
+ * should come before any stream capture.  All calls share the array: calls
+ * that overlap on the GPU (other streams, other contexts) race on it.
+ * Returns the frames produced, 0 on failure. */
+FFT_CFFI_API size_t fftfree_execute_complex_batched_noalloc(void* handle, const float* in_real,
+                                                           const float* in_imag, size_t frames,
+                                                           float* out_pcm, size_t max_frames);
+
 /* Test hook of the recovery coordinator (fft_cffi.cpp:954-982): runs the
  * host-side dropout / restore / split decisions for one batch of `frames`
  * frames, invoking the registered restore observer as the recovery path
