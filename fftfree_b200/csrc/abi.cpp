@@ -263,6 +263,7 @@ static void setup_device(FftContext* c) {
   FFB_CHECK(cudaStreamCreateWithFlags(&c->own_stream, cudaStreamNonBlocking));
   c->stream = c->own_stream;
   (void)twiddle_pyramid(ilog2((size_t)std::max(c->N, 1)) + 1, c->stream);
+  if (!twiddle_pass_tables(c->stream)) throw std::runtime_error("twiddle tables");
   upload_windows(c);
 }
 

@@ -13,6 +13,13 @@
 // Input layout: v[i] = x[t + i*T];  output layout: v[i] = X[t + i*T]
 // (natural order, no final exchange).
 //
+// sm_100a specifics: complex additions use the packed FP32x2 instructions
+// (__fadd2_rn / __ffma2_rn, one instruction per complex add); the shared
+// tile is padded by one float2 per 16 (conflict-free for every pass
+// pattern) so that each element's offset from a per-thread base is a
+// compile-time constant; per-pass twiddles come from r-major tables
+// (coalesced loads with immediate offsets).
+//
 // This replaces the reference's radix-2 executors (eigen_fft.hpp:2655-3100
 // Cooley-Tukey, :3227-3623 Stockham): the transform computed is the same DFT
 // (forward sign -1), the stage structure is radix 4/8/16.
@@ -21,34 +28,49 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <utility>
+
 namespace ffb {
 
 // ---------------------------------------------------------------- complex
-__device__ __forceinline__ float2 cadd(float2 a, float2 b) { return make_float2(a.x + b.x, a.y + b.y); }
-__device__ __forceinline__ float2 csub(float2 a, float2 b) { return make_float2(a.x - b.x, a.y - b.y); }
+__device__ __forceinline__ float2 cadd(float2 a, float2 b) { return __fadd2_rn(a, b); }
+__device__ __forceinline__ float2 csub(float2 a, float2 b) {
+  return __ffma2_rn(b, make_float2(-1.f, -1.f), a);  // a - b, one rounding
+}
 __device__ __forceinline__ float2 cmul(float2 a, float2 b) {
   return make_float2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
 }
 __device__ __forceinline__ float2 cconj(float2 a) { return make_float2(a.x, -a.y); }
-__device__ __forceinline__ float2 cscale(float2 a, float s) { return make_float2(a.x * s, a.y * s); }
+__device__ __forceinline__ float2 cscale(float2 a, float s) { return __fmul2_rn(a, make_float2(s, s)); }
 // -i * a
 __device__ __forceinline__ float2 mul_mi(float2 a) { return make_float2(a.y, -a.x); }
 
 // ---------------------------------------------------------------- twiddles
-// Twiddle pyramid in global memory: level L (0 <= L <= TW_MAX_LOG) holds
-// w_L[e] = exp(-2*pi*i*e / 2^L), e < 2^L, at offset 2^L - 1.  Built on the
-// host in FP64 with octant symmetry (exact 0 / +-1 at the quarter points).
+// Two FP64-built tables in global memory (host side: kernels.cu):
+//  * pyramid: level L (0 <= L <= 18) holds w_L[e] = exp(-2*pi*i*e / 2^L),
+//    e < 2^L, at offset 2^L - 1 (untangle and four-step twiddles);
+//  * pass tables: for radix R = 2^lr and sub-size Ns = 2^lns the R-1 rows
+//    w[(r-1)*Ns + k] = exp(-2*pi*i*k*r / (Ns*R)), k < Ns.
+constexpr int kPassMaxLog = 12;  // largest log2(Ns) of a single-pass kernel
+
+__host__ __device__ constexpr long long pass_table_offset(int lr, int lns) {
+  long long off = 0;
+  for (int l = 1; l < lr; ++l) off += (long long)((1 << l) - 1) * ((1LL << (kPassMaxLog + 1)) - 1);
+  return off + (long long)((1 << lr) - 1) * ((1LL << lns) - 1);
+}
+constexpr long long pass_table_size() { return pass_table_offset(5, 0); }
+
 struct Twiddles {
-  const float2* __restrict__ base;
+  const float2* __restrict__ pyr;
+  const float2* __restrict__ pass;
 };
 
 __device__ __forceinline__ float2 tw_get(const Twiddles& tw, int L, unsigned e) {
-  return __ldg(tw.base + ((1u << L) - 1u) + (e & ((1u << L) - 1u)));
+  return __ldg(tw.pyr + ((1u << L) - 1u) + (e & ((1u << L) - 1u)));
 }
 
-// 16th roots of unity (cos, sin of 2*pi*m/16), m = 0..15.
+// exp(-2*pi*i*m/16)
 __device__ __forceinline__ float2 w16(int m) {
-  // exp(-2*pi*i*m/16) = (cos, -sin)
   constexpr float c1 = 0.92387953251128675613f;  // cos(pi/8)
   constexpr float s1 = 0.38268343236508977173f;  // sin(pi/8)
   constexpr float h = 0.70710678118654752440f;   // sqrt(1/2)
@@ -73,74 +95,73 @@ __device__ __forceinline__ float2 w16(int m) {
 }
 
 // ---------------------------------------------------------------- small DFTs
-// Forward DFT of R points held in v[stride*0 .. stride*(R-1)], in place,
-// natural order in and out.
-template <int R, int S = 1>
+// Forward DFT of R points held in v[0 .. R-1], in place, natural order.
+template <int R>
 struct Dft;
 
-template <int S>
-struct Dft<1, S> {
+template <>
+struct Dft<1> {
   __device__ __forceinline__ static void run(float2*) {}
 };
 
-template <int S>
-struct Dft<2, S> {
+template <>
+struct Dft<2> {
   __device__ __forceinline__ static void run(float2* v) {
     const float2 a = v[0];
-    v[0] = cadd(a, v[S]);
-    v[S] = csub(a, v[S]);
+    v[0] = cadd(a, v[1]);
+    v[1] = csub(a, v[1]);
   }
 };
 
-template <int S>
-struct Dft<4, S> {
+template <>
+struct Dft<4> {
   __device__ __forceinline__ static void run(float2* v) {
-    const float2 a0 = cadd(v[0], v[2 * S]);
-    const float2 a1 = csub(v[0], v[2 * S]);
-    const float2 a2 = cadd(v[S], v[3 * S]);
-    const float2 a3 = mul_mi(csub(v[S], v[3 * S]));
+    const float2 a0 = cadd(v[0], v[2]);
+    const float2 a1 = csub(v[0], v[2]);
+    const float2 a2 = cadd(v[1], v[3]);
+    const float2 d = csub(v[1], v[3]);
     v[0] = cadd(a0, a2);
-    v[2 * S] = csub(a0, a2);
-    v[S] = cadd(a1, a3);
-    v[3 * S] = csub(a1, a3);
+    v[2] = csub(a0, a2);
+    // a1 -+ i*d
+    v[1] = make_float2(a1.x + d.y, a1.y - d.x);
+    v[3] = make_float2(a1.x - d.y, a1.y + d.x);
   }
 };
 
-template <int S>
-struct Dft<8, S> {
+template <>
+struct Dft<8> {
   __device__ __forceinline__ static void run(float2* v) {
     // 2 x 4: DFT4 over even and odd points, then radix-2 combine.
-    float2 e[4] = {v[0], v[2 * S], v[4 * S], v[6 * S]};
-    float2 o[4] = {v[S], v[3 * S], v[5 * S], v[7 * S]};
-    Dft<4, 1>::run(e);
-    Dft<4, 1>::run(o);
+    float2 e[4] = {v[0], v[2], v[4], v[6]};
+    float2 o[4] = {v[1], v[3], v[5], v[7]};
+    Dft<4>::run(e);
+    Dft<4>::run(o);
     constexpr float h = 0.70710678118654752440f;
-    const float2 o1 = make_float2((o[1].x + o[1].y) * h, (o[1].y - o[1].x) * h);
-    const float2 o2 = mul_mi(o[2]);
-    const float2 o3 = make_float2((o[3].y - o[3].x) * h, -(o[3].x + o[3].y) * h);
+    const float2 t1 = make_float2((o[1].x + o[1].y) * h, (o[1].y - o[1].x) * h);
+    const float2 t3 = make_float2((o[3].y - o[3].x) * h, -(o[3].x + o[3].y) * h);
     v[0] = cadd(e[0], o[0]);
-    v[4 * S] = csub(e[0], o[0]);
-    v[S] = cadd(e[1], o1);
-    v[5 * S] = csub(e[1], o1);
-    v[2 * S] = cadd(e[2], o2);
-    v[6 * S] = csub(e[2], o2);
-    v[3 * S] = cadd(e[3], o3);
-    v[7 * S] = csub(e[3], o3);
+    v[4] = csub(e[0], o[0]);
+    v[1] = cadd(e[1], t1);
+    v[5] = csub(e[1], t1);
+    v[2] = make_float2(e[2].x + o[2].y, e[2].y - o[2].x);
+    v[6] = make_float2(e[2].x - o[2].y, e[2].y + o[2].x);
+    v[3] = cadd(e[3], t3);
+    v[7] = csub(e[3], t3);
   }
 };
 
-template <int S>
-struct Dft<16, S> {
+template <>
+struct Dft<16> {
   __device__ __forceinline__ static void run(float2* v) {
     // 4 x 4: X[k1 + 4 k2] = sum_n2 w4^(n2 k2) w16^(n2 k1) sum_n1 x[4 n1 + n2] w4^(n1 k1)
     float2 a[16];
 #pragma unroll
     for (int n2 = 0; n2 < 4; ++n2) {
-      a[4 * n2 + 0] = v[(n2)*S];
-      a[4 * n2 + 1] = v[(4 + n2) * S];
-      a[4 * n2 + 2] = v[(8 + n2) * S];
-      a[4 * n2 + 3] = v[(12 + n2) * S];
-      Dft<4, 1>::run(a + 4 * n2);
+      a[4 * n2 + 0] = v[n2];
+      a[4 * n2 + 1] = v[4 + n2];
+      a[4 * n2 + 2] = v[8 + n2];
+      a[4 * n2 + 3] = v[12 + n2];
+      Dft<4>::run(a + 4 * n2);
     }
 #pragma unroll
     for (int n2 = 1; n2 < 4; ++n2) {
@@ -154,11 +175,11 @@ struct Dft<16, S> {
 #pragma unroll
     for (int k1 = 0; k1 < 4; ++k1) {
       float2 b[4] = {a[k1], a[4 + k1], a[8 + k1], a[12 + k1]};
-      Dft<4, 1>::run(b);
-      v[(k1)*S] = b[0];
-      v[(k1 + 4) * S] = b[1];
-      v[(k1 + 8) * S] = b[2];
-      v[(k1 + 12) * S] = b[3];
+      Dft<4>::run(b);
+      v[k1] = b[0];
+      v[k1 + 4] = b[1];
+      v[k1 + 8] = b[2];
+      v[k1 + 12] = b[3];
     }
   }
 };
@@ -170,23 +191,81 @@ struct Sched {
   static constexpr int M = 1 << LOGM;
   static constexpr int LOGR = (LOGR_ < LOGM) ? LOGR_ : LOGM;
   static constexpr int R = 1 << LOGR;
-  static constexpr int T = M / R;                        // threads per transform
-  static constexpr int NFULL = (LOGR > 0) ? LOGM / LOGR : 0;  // full radix-R passes
-  static constexpr int LOGR0 = (LOGR > 0) ? LOGM % LOGR : 0;  // leading small pass
+  static constexpr int T = M / R;                              // threads per transform
+  static constexpr int NFULL = (LOGR > 0) ? LOGM / LOGR : 0;   // full radix-R passes
+  static constexpr int LOGR0 = (LOGR > 0) ? LOGM % LOGR : 0;   // leading small pass
+  static constexpr int SMEM = M + (M >> 4) + 2;                // padded tile (float2), index M included
 };
 
-// XOR swizzle of a shared-memory float2 index: flips the low 4 bits with the
-// next 4.  A bijection on every aligned block of 16, it makes the strided
-// Stockham write patterns and the unit-stride reads bank-conflict free.
-__device__ __forceinline__ int sw(int a) { return a ^ ((a >> 4) & 15); }
+// Padded shared-memory index: one float2 of padding per 16.
+__device__ __forceinline__ int pidx(int a) { return a + (a >> 4); }
 
-// The engine.  `sm` is this group's tile of M float2; `bar` synchronises all
-// groups of the block (every thread of the block calls the engine).
+// v[i] <- tile[t + i*T]
+template <class S>
+__device__ __forceinline__ void tile_read(float2 (&v)[S::R], int t, const float2* sm) {
+  if constexpr (S::T % 16 == 0) {
+    const float2* b = sm + pidx(t);
+#pragma unroll
+    for (int i = 0; i < S::R; ++i) v[i] = b[i * S::T + ((i * S::T) >> 4)];
+  } else {
+#pragma unroll
+    for (int i = 0; i < S::R; ++i) v[i] = sm[pidx(t + i * S::T)];
+  }
+}
+
+// tile[t + i*T] <- v[i]
+template <class S>
+__device__ __forceinline__ void tile_write_natural(const float2 (&v)[S::R], int t, float2* sm) {
+  if constexpr (S::T % 16 == 0) {
+    float2* b = sm + pidx(t);
+#pragma unroll
+    for (int i = 0; i < S::R; ++i) b[i * S::T + ((i * S::T) >> 4)] = v[i];
+  } else {
+#pragma unroll
+    for (int i = 0; i < S::R; ++i) sm[pidx(t + i * S::T)] = v[i];
+  }
+}
+
+template <class S, int P>
+__device__ __forceinline__ void stockham_pass(float2 (&v)[S::R], int t, float2* sm, const Twiddles& tw) {
+  constexpr int R = S::R, LR = S::LOGR;
+  constexpr int LNS = S::LOGR0 + P * LR;
+  constexpr int NS = 1 << LNS;
+  const int k = t & (NS - 1);
+  if constexpr (LNS > 0) {
+    const float2* w = tw.pass + pass_table_offset(LR, LNS) + k;
+#pragma unroll
+    for (int r = 1; r < R; ++r) v[r] = cmul(v[r], __ldg(w + (r - 1) * NS));
+  }
+  Dft<R>::run(v);
+  if constexpr (P != S::NFULL - 1) {
+    const int base = ((t >> LNS) << (LNS + LR)) + k;
+    if constexpr (NS >= 16 || LNS + LR >= 4) {
+      // (base + r*NS) >> 4 == (base >> 4) + (r*NS >> 4) for these patterns
+      float2* b = sm + pidx(base);
+#pragma unroll
+      for (int r = 0; r < R; ++r) b[r * NS + ((r * NS) >> 4)] = v[r];
+    } else {
+#pragma unroll
+      for (int r = 0; r < R; ++r) sm[pidx(base + r * NS)] = v[r];
+    }
+    __syncthreads();
+    tile_read<S>(v, t, sm);
+    __syncthreads();
+  }
+}
+
+template <class S, int... P>
+__device__ __forceinline__ void run_passes(float2 (&v)[S::R], int t, float2* sm, const Twiddles& tw,
+                                           std::integer_sequence<int, P...>) {
+  (stockham_pass<S, P>(v, t, sm, tw), ...);
+}
+
+// The engine.  `sm` is this group's padded tile (S::SMEM float2); every
+// thread of the block calls the engine (it contains block barriers).
 template <class S>
 __device__ __forceinline__ void fft_engine(float2 (&v)[S::R], int t, float2* sm, const Twiddles& tw) {
-  constexpr int M = S::M, R = S::R, T = S::T;
-  int Ns = 1;
-  int logNs = 0;
+  constexpr int R = S::R, T = S::T;
   if constexpr (S::LOGR0 > 0) {
     constexpr int r0 = 1 << S::LOGR0;
     constexpr int Q = R / r0;
@@ -195,39 +274,16 @@ __device__ __forceinline__ void fft_engine(float2 (&v)[S::R], int t, float2* sm,
       float2 u[r0];
 #pragma unroll
       for (int r = 0; r < r0; ++r) u[r] = v[q + r * Q];
-      Dft<r0, 1>::run(u);
+      Dft<r0>::run(u);
       const int j = t + q * T;
 #pragma unroll
-      for (int r = 0; r < r0; ++r) sm[sw(j * r0 + r)] = u[r];
+      for (int r = 0; r < r0; ++r) sm[pidx(j * r0 + r)] = u[r];
     }
     __syncthreads();
-#pragma unroll
-    for (int i = 0; i < R; ++i) v[i] = sm[sw(t + i * T)];
+    tile_read<S>(v, t, sm);
     __syncthreads();
-    Ns = r0;
-    logNs = S::LOGR0;
   }
-#pragma unroll
-  for (int p = 0; p < S::NFULL; ++p) {
-    const int k = t & (Ns - 1);
-    if (p > 0 || S::LOGR0 > 0) {
-      const int L = logNs + S::LOGR;
-#pragma unroll
-      for (int r = 1; r < R; ++r) v[r] = cmul(v[r], tw_get(tw, L, (unsigned)(k * r)));
-    }
-    Dft<R, 1>::run(v);
-    if (p == S::NFULL - 1) break;
-    const int base = ((t >> logNs) << (logNs + S::LOGR)) + k;
-#pragma unroll
-    for (int r = 0; r < R; ++r) sm[sw(base + r * Ns)] = v[r];
-    __syncthreads();
-#pragma unroll
-    for (int i = 0; i < R; ++i) v[i] = sm[sw(t + i * T)];
-    __syncthreads();
-    Ns <<= S::LOGR;
-    logNs += S::LOGR;
-  }
-  (void)M;
+  run_passes<S>(v, t, sm, tw, std::make_integer_sequence<int, S::NFULL>{});
 }
 
 }  // namespace ffb

@@ -12,6 +12,19 @@
 namespace ffb {
 
 // ------------------------------------------------------------------ hooks
+// |z| as sqrt(x^2 + y^2): the squares summed with one rounding (fma), then
+// the correctly rounded square root; magnitudes whose squares could
+// overflow fall back to hypotf.
+__device__ __forceinline__ float cabs_fast(float x, float y) {
+  const float s = fmaf(x, x, y * y);
+  if (s < 1e36f) return __fsqrt_rn(s);
+  return hypotf(x, y);
+}
+
+__device__ __forceinline__ bool any_post(const PostFlags& pf) {
+  return (pf.r2c_half | pf.polar | pf.reduce | pf.clear_imag) != 0;
+}
+
 __device__ __forceinline__ float2 post_hook(float2 X, int k, int N, const PostFlags& pf) {
   // eigen_fft.hpp:2544-2595.  Polar/reduce apply below `upper`; above it the
   // R2C half branch has already zeroed the value, and (0,0) is a fixed point
@@ -21,11 +34,11 @@ __device__ __forceinline__ float2 post_hook(float2 X, int k, int N, const PostFl
     else if (k == 0 || k == (N >> 1)) X.y = 0.f;
   }
   if (pf.polar) {
-    const float m = hypotf(X.x, X.y);
+    const float m = cabs_fast(X.x, X.y);
     const float ph = atan2f(X.y, X.x);
     X = make_float2(m, ph);
   } else if (pf.reduce) {
-    X = make_float2(hypotf(X.x, X.y), 0.f);
+    X = make_float2(cabs_fast(X.x, X.y), 0.f);
   } else if (pf.clear_imag) {
     X.y = 0.f;
   }
@@ -38,32 +51,63 @@ __device__ __forceinline__ float2 polar_to_complex(float2 u) {
   return make_float2(u.x * c, u.x * s);
 }
 
+__device__ __forceinline__ bool aligned8(const void* p) { return (reinterpret_cast<uintptr_t>(p) & 7) == 0; }
+
 // ------------------------------------------------------------------ STFT IO
 struct StftIO {
   StftArgs a;
   int logN;
 
-  __device__ __forceinline__ float sample(long long f, int n) const {
-    // fft_cffi.cpp:765-791 framing (+ Cooley-Tukey C2R half mirror of the
-    // pre-hook, eigen_fft.hpp:2523-2528, which on real frames is x[N-n]=x[n]).
-    if (a.mirror && n > (a.N >> 1)) n = a.N - n;
+  template <class S>
+  __device__ __forceinline__ void load(long long f, int t, float2 (&v)[S::R], float2*, const Twiddles&) const {
+    if (f >= a.frames) {
+#pragma unroll
+      for (int i = 0; i < S::R; ++i) v[i] = make_float2(0.f, 0.f);
+      return;
+    }
+    // fft_cffi.cpp:765-791 framing: frame f covers pcm[f*H .. f*H + W), zero
+    // beyond the signal end and from W up to N; Cooley-Tukey C2R half adds the
+    // pre-hook's mirror (eigen_fft.hpp:2523-2528), x[N-n] = x[n] on real frames.
     const long long start = f * (long long)a.H;
     long long cnt = a.pcm_len - start;
     if (cnt > a.W) cnt = a.W;
-    if ((long long)n >= cnt) return 0.f;
-    const float s = __ldg(a.pcm + start + n);
-    return a.win ? s * __ldg(a.win + n) : s;
-  }
-
-  template <class S>
-  __device__ __forceinline__ void load(long long f, int t, float2 (&v)[S::R], const Twiddles&) const {
-    const bool ok = f < a.frames;
+    const float* src = a.pcm + start;
+    if (a.N == 1) {
+      const float s = (cnt > 0) ? __ldg(src) : 0.f;
+#pragma unroll
+      for (int i = 0; i < S::R; ++i) v[i] = make_float2(a.win && cnt > 0 ? s * __ldg(a.win) : s, 0.f);
+      return;
+    }
+    if (!a.mirror && cnt == a.N && aligned8(src) && (!a.win || aligned8(a.win))) {
+      // whole frame present: z[m] = (x[2m], x[2m+1]) as one 8-byte load
+      const float2* s2 = reinterpret_cast<const float2*>(src);
+      const float2* w2 = reinterpret_cast<const float2*>(a.win);
+#pragma unroll
+      for (int i = 0; i < S::R; ++i) {
+        const int m = t + i * S::T;
+        float2 z = __ldg(s2 + m);
+        if (w2) z = __fmul2_rn(z, __ldg(w2 + m));
+        v[i] = z;
+      }
+      return;
+    }
+    const int half = a.N >> 1;
 #pragma unroll
     for (int i = 0; i < S::R; ++i) {
       const int m = t + i * S::T;
-      if (!ok) { v[i] = make_float2(0.f, 0.f); continue; }
-      if (a.N == 1) v[i] = make_float2(sample(f, 0), 0.f);
-      else v[i] = make_float2(sample(f, 2 * m), sample(f, 2 * m + 1));
+      float x[2];
+#pragma unroll
+      for (int j = 0; j < 2; ++j) {
+        int n = 2 * m + j;
+        if (a.mirror && n > half) n = a.N - n;
+        float s = 0.f;
+        if ((long long)n < cnt) {
+          s = __ldg(src + n);
+          if (a.win) s *= __ldg(a.win + n);
+        }
+        x[j] = s;
+      }
+      v[i] = make_float2(x[0], x[1]);
     }
   }
 
@@ -71,12 +115,13 @@ struct StftIO {
   __device__ __forceinline__ void store(long long f, int t, float2 (&v)[S::R], float2* sm,
                                         const Twiddles& tw) const {
     constexpr int M = S::M;
-#pragma unroll
-    for (int i = 0; i < S::R; ++i) sm[sw(t + i * S::T)] = v[i];
+    tile_write_natural<S>(v, t, sm);
     __syncthreads();
     if (f >= a.frames) return;
     const int N = a.N;
     const long long ob = f * a.out_stride;
+    const float inv_n = 1.0f / (float)N;
+    const bool mag_is_re = a.pf.reduce || (a.pf.polar && a.mag_from_real);
     for (int k = t; k < a.out_bins; k += S::T) {
       int kk = k;
       bool cj = false;
@@ -87,22 +132,22 @@ struct StftIO {
       } else {
         // Real-input untangle of the N/2-point transform Z of z[m] = x[2m] + i x[2m+1]:
         // X[k] = E + w^k O,  E = (Z[k] + conj Z[M-k]) / 2,  O = -i (Z[k] - conj Z[M-k]) / 2
-        const float2 zk = sm[sw(kk & (M - 1))];
-        const float2 zm = sm[sw((M - kk) & (M - 1))];
+        const float2 zk = sm[pidx(kk & (M - 1))];
+        const float2 zm = sm[pidx((M - kk) & (M - 1))];
         const float2 E = make_float2(0.5f * (zk.x + zm.x), 0.5f * (zk.y - zm.y));
         const float2 D = make_float2(zk.x - zm.x, zk.y + zm.y);
         const float2 O = make_float2(0.5f * D.y, -0.5f * D.x);
         X = cadd(E, cmul(tw_get(tw, logN, (unsigned)kk), O));
       }
       if (cj) X = cconj(X);
-      if (a.inverse) X = cscale(cconj(X), 1.0f / (float)N);
+      if (a.inverse) X = make_float2(X.x * inv_n, -X.y * inv_n);
       // Real input: DC and Nyquist are exactly real (imag +0), as in the
       // reference's radix-2 executors.
       if (kk == 0 || 2 * kk == N) X.y = 0.f;
       X = post_hook(X, k, N, a.pf);
       a.out_re[ob + k] = X.x;
       a.out_im[ob + k] = X.y;
-      a.out_mag[ob + k] = (a.mag_from_real && a.pf.polar) ? X.x : hypotf(X.x, X.y);
+      a.out_mag[ob + k] = mag_is_re ? X.x : cabs_fast(X.x, X.y);
     }
   }
 };
@@ -111,8 +156,7 @@ struct StftIO {
 struct C2cIO {
   C2cArgs a;
 
-  __device__ __forceinline__ float2 elem(long long b, int n) const {
-    const float2* col = a.in + b * (long long)a.N;
+  __device__ __forceinline__ float2 elem(const float2* col, int n) const {
     if (a.pre == 1) {  // eigen_fft.hpp:2493-2502
       float2 u = col[n];
       u.y = 0.f;
@@ -131,12 +175,21 @@ struct C2cIO {
   }
 
   template <class S>
-  __device__ __forceinline__ void load(long long b, int t, float2 (&v)[S::R], const Twiddles&) const {
-    const bool ok = b < a.batch;
+  __device__ __forceinline__ void load(long long b, int t, float2 (&v)[S::R], float2*, const Twiddles&) const {
+    if (b >= a.batch) {
 #pragma unroll
-    for (int i = 0; i < S::R; ++i) {
-      float2 u = ok ? elem(b, t + i * S::T) : make_float2(0.f, 0.f);
-      v[i] = a.inverse ? cconj(u) : u;  // inverse = conj . forward . conj
+      for (int i = 0; i < S::R; ++i) v[i] = make_float2(0.f, 0.f);
+      return;
+    }
+    const float2* col = a.in + b * (long long)a.N;
+    // inverse = conj . forward . conj
+    const float2 sg = make_float2(1.f, a.inverse ? -1.f : 1.f);
+    if (a.pre == 0) {
+#pragma unroll
+      for (int i = 0; i < S::R; ++i) v[i] = __fmul2_rn(col[t + i * S::T], sg);
+    } else {
+#pragma unroll
+      for (int i = 0; i < S::R; ++i) v[i] = __fmul2_rn(elem(col, t + i * S::T), sg);
     }
   }
 
@@ -145,13 +198,17 @@ struct C2cIO {
                                         const Twiddles&) const {
     if (b >= a.batch) return;
     float2* col = a.out + b * (long long)a.N;
-    const float scale = 1.0f / (float)a.N;
+    const float sc = a.inverse ? 1.0f / (float)a.N : 1.0f;
+    const float2 sg = make_float2(sc, a.inverse ? -sc : sc);
+    if (!any_post(a.pf)) {
 #pragma unroll
-    for (int i = 0; i < S::R; ++i) {
-      const int k = t + i * S::T;
-      float2 X = v[i];
-      if (a.inverse) X = cscale(cconj(X), scale);
-      col[k] = post_hook(X, k, a.N, a.pf);
+      for (int i = 0; i < S::R; ++i) col[t + i * S::T] = __fmul2_rn(v[i], sg);
+    } else {
+#pragma unroll
+      for (int i = 0; i < S::R; ++i) {
+        const int k = t + i * S::T;
+        col[k] = post_hook(__fmul2_rn(v[i], sg), k, a.N, a.pf);
+      }
     }
   }
 };
@@ -187,7 +244,7 @@ struct CplxBatchIO {
   }
 
   template <class S>
-  __device__ __forceinline__ void load(long long f, int t, float2 (&v)[S::R], const Twiddles&) const {
+  __device__ __forceinline__ void load(long long f, int t, float2 (&v)[S::R], float2*, const Twiddles&) const {
     const bool ok = f < a.frames;
 #pragma unroll
     for (int i = 0; i < S::R; ++i) {
@@ -215,6 +272,82 @@ struct CplxBatchIO {
   }
 };
 
+// Hermitian (C2R + half spectrum) complex batch as an N/2-point transform.
+// With X[0..M] (M = N/2) the half spectrum of a real x,
+//   E[m] = (X[m] + conj X[M-m]) / 2,  O[m] = (X[m] - conj X[M-m]) e^{+2 pi i m/N} / 2
+// are the spectra of x[2m] and x[2m+1], so z = IDFT_M(E + i O) gives
+// x[2m] = Re z[m], x[2m+1] = Im z[m].  A forward context transforms the
+// conjugate spectrum instead and scales by N.  Each bin is read and (for
+// Cooley-Tukey polar input) converted once, through the shared tile.
+struct C2rHalfIO {
+  CplxBatchArgs a;
+  int logN;
+
+  template <class S>
+  __device__ __forceinline__ void load(long long f, int t, float2 (&v)[S::R], float2* sm,
+                                       const Twiddles& tw) const {
+    constexpr int M = S::M;
+    const bool ok = f < a.frames;
+    if (ok) {
+      const float* re = a.in_re + f * (long long)a.bins;
+      const float* im = a.in_im + f * (long long)a.bins;
+      const float cs = a.inverse ? 1.f : -1.f;  // forward: conjugate spectrum
+      for (int k = t; k <= M; k += S::T) {
+        float2 u = make_float2(__ldg(re + k), __ldg(im + k));
+        if (k == 0 || k == M) u.y = 0.f;  // fft_cffi.cpp:1073-1078
+        if (a.ct_pre == 2 && a.polar_in) {  // eigen_fft.hpp:2511-2522
+          u = polar_to_complex(u);
+          if (k == 0 || k == M) u.y = 0.f;
+        }
+        u.y *= cs;
+        sm[pidx(k)] = u;
+      }
+    }
+    __syncthreads();
+#pragma unroll
+    for (int i = 0; i < S::R; ++i) {
+      const int m = t + i * S::T;
+      float2 z = make_float2(0.f, 0.f);
+      if (ok) {
+        const float2 xk = sm[pidx(m)];
+        const float2 xm = sm[pidx(M - m)];
+        const float2 E = make_float2(0.5f * (xk.x + xm.x), 0.5f * (xk.y - xm.y));
+        const float2 D = make_float2(0.5f * (xk.x - xm.x), 0.5f * (xk.y + xm.y));
+        const float2 O = cmul(D, cconj(tw_get(tw, logN, (unsigned)m)));
+        z = make_float2(E.x - O.y, E.y + O.x);  // E + i O
+      }
+      v[i] = cconj(z);  // IDFT via conj . DFT . conj
+    }
+    __syncthreads();  // the engine reuses the tile
+  }
+
+  template <class S>
+  __device__ __forceinline__ void store(long long f, int t, float2 (&v)[S::R], float2*,
+                                        const Twiddles&) const {
+    if (f >= a.frames) return;
+    constexpr int M = S::M;
+    const float scale = a.inverse ? 1.0f / (float)M : 2.0f;  // forward: N/M
+    const bool absval = a.pf.polar || a.pf.reduce;           // post hook on a real value
+    float* o = a.out + f * (long long)a.N;
+    const bool vec = aligned8(o) && (!a.synth || aligned8(a.synth));
+#pragma unroll
+    for (int i = 0; i < S::R; ++i) {
+      const int m = t + i * S::T;
+      float x0 = v[i].x * scale, x1 = -v[i].y * scale;
+      if (absval) { x0 = fabsf(x0); x1 = fabsf(x1); }
+      if (vec) {
+        float2 s = make_float2(x0, x1);
+        if (a.synth) s = __fmul2_rn(s, __ldg(reinterpret_cast<const float2*>(a.synth) + m));
+        reinterpret_cast<float2*>(o)[m] = s;
+      } else {
+        if (a.synth) { x0 *= __ldg(a.synth + 2 * m); x1 *= __ldg(a.synth + 2 * m + 1); }
+        o[2 * m] = x0;
+        o[2 * m + 1] = x1;
+      }
+    }
+  }
+};
+
 // ------------------------------------------------------------------ kernel
 template <class S>
 struct Launch {
@@ -230,9 +363,9 @@ k_fft(IO io, Twiddles tw) {
   const int g = threadIdx.x / T;
   const int t = threadIdx.x - g * T;
   const long long b = (long long)blockIdx.x * Launch<S>::G + g;
-  float2* sm = smem + g * S::M;
+  float2* sm = smem + g * S::SMEM;
   float2 v[S::R];
-  io.template load<S>(b, t, v, tw);
+  io.template load<S>(b, t, v, sm, tw);
   fft_engine<S>(v, t, sm, tw);
   io.template store<S>(b, t, v, sm, tw);
 }
@@ -243,13 +376,13 @@ static cudaError_t run(const IO& io, long long nbatch, cudaStream_t st, uint64_t
   if (nbatch <= 0) return cudaSuccess;
   const long long grid = (nbatch + L::G - 1) / L::G;
   if (grid > 0x7fffffffLL) return cudaErrorInvalidValue;
-  const size_t smem = (size_t)L::G * S::M * sizeof(float2);
+  const size_t smem = (size_t)L::G * S::SMEM * sizeof(float2);
   if (smem > 48 * 1024) {
     cudaError_t e = cudaFuncSetAttribute(k_fft<S, IO>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          (int)smem);
     if (e != cudaSuccess) return e;
   }
-  Twiddles tw{twiddle_pyramid(0, st)};
+  Twiddles tw{twiddle_pyramid(0, st), twiddle_pass_tables(st)};
   k_fft<S, IO><<<(unsigned)grid, L::BLOCK, smem, st>>>(io, tw);
   if (launches) ++*launches;
   return cudaGetLastError();
@@ -328,8 +461,13 @@ cudaError_t launch_c2c(const C2cArgs& a, int logr, cudaStream_t s, uint64_t* lau
 }
 
 cudaError_t launch_cplx_batch(const CplxBatchArgs& a, int logr, cudaStream_t s, uint64_t* launches) {
+  const int lg = ilog2i(a.N);
+  if (a.c2r_half && a.N >= 4) {
+    C2rHalfIO io{a, lg};
+    return dispatch(io, lg - 1, logr, a.frames, s, launches);
+  }
   CplxBatchIO io{a};
-  return dispatch(io, ilog2i(a.N), logr, a.frames, s, launches);
+  return dispatch(io, lg, logr, a.frames, s, launches);
 }
 
 // ------------------------------------------------------------------ OLA
@@ -450,6 +588,43 @@ const float2* twiddle_pyramid(int max_log, cudaStream_t stream) {
   p.dev = d;
   p.max_log = want;
   return p.dev;
+}
+
+
+namespace {
+std::vector<float2*> g_pass;  // per device, guarded by g_tw_mu
+}
+
+// Per-pass twiddle tables (layout in fft_engine.cuh, pass_table_offset):
+// w[(r-1)*Ns + k] = exp(-2 pi i k r / (Ns R)), built in FP64 with the same
+// octant symmetry as the pyramid.
+const float2* twiddle_pass_tables(cudaStream_t stream) {
+  int dev = 0;
+  cudaGetDevice(&dev);
+  std::lock_guard<std::mutex> lk(g_tw_mu);
+  if ((int)g_pass.size() <= dev) g_pass.resize(dev + 1, nullptr);
+  if (g_pass[dev]) return g_pass[dev];
+  const long long total = pass_table_size();
+  std::vector<float2> host((size_t)total);
+  for (int lr = 1; lr <= 4; ++lr) {
+    const int R = 1 << lr;
+    for (int lns = 0; lns <= kPassMaxLog; ++lns) {
+      const long long Ns = 1LL << lns;
+      const long long off = pass_table_offset(lr, lns);
+      for (int r = 1; r < R; ++r)
+        for (long long k = 0; k < Ns; ++k) {
+          double c, s;
+          octant_value(k * r, lns + lr, &c, &s);
+          host[(size_t)(off + (r - 1) * Ns + k)] = make_float2((float)c, (float)s);
+        }
+    }
+  }
+  float2* d = nullptr;
+  if (cudaMalloc(&d, host.size() * sizeof(float2)) != cudaSuccess) return nullptr;
+  cudaMemcpyAsync(d, host.data(), host.size() * sizeof(float2), cudaMemcpyHostToDevice, stream);
+  cudaStreamSynchronize(stream);
+  g_pass[dev] = d;
+  return d;
 }
 
 }  // namespace ffb

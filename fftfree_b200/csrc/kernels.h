@@ -72,6 +72,8 @@ struct OlaArgs {
 
 // Twiddle pyramid (levels 0..max_log) on the current device.
 const float2* twiddle_pyramid(int max_log, cudaStream_t stream);
+// Per-pass twiddle tables of the single-pass engine on the current device.
+const float2* twiddle_pass_tables(cudaStream_t stream);
 
 // Pick the single-pass radix (log2) for a transform of 2^logm points;
 // `requested_log` (2..4) is honoured when valid.  Returns -1 if the size
