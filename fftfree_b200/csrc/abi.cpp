@@ -328,11 +328,7 @@ static void run_stft(FftContext* c, const float* pcm, size_t pcm_len, size_t fra
   a.out_re = o_re.dev;
   a.out_im = o_im.dev;
   a.out_mag = o_mag.dev;
-  const int lg = ilog2((size_t)c->N);
-  const int logm = (c->N == 1) ? 0 : lg - 1;
-  const int logr = choose_logr(logm, c->logr_req);
-  if (logr < 0) throw std::runtime_error("transform size not supported");
-  FFB_CHECK(launch_stft(a, logr, c->stream, &c->launches));
+  FFB_CHECK(launch_stft(a, c->logr_req, c->stream, &c->launches));
   finish_out(c, o_re);
   finish_out(c, o_im);
   finish_out(c, o_mag);
@@ -371,9 +367,7 @@ static void run_complex_batch(FftContext* c, const float* in_re, const float* in
   a.synth = c->windows_enabled ? static_cast<const float*>(c->d_synthesis.p) : nullptr;
   float* frames_out = c->apply_ola ? static_cast<float*>(c->d_frames.get(outn * sizeof(float))) : o.dev;
   a.out = frames_out;
-  const int logr = choose_logr(ilog2((size_t)N), c->logr_req);
-  if (logr < 0) throw std::runtime_error("transform size not supported");
-  FFB_CHECK(launch_cplx_batch(a, logr, c->stream, &c->launches));
+  FFB_CHECK(launch_cplx_batch(a, c->logr_req, c->stream, &c->launches));
   if (raw_frames) {
     // Frames the recovery coordinator gave up on keep the restored
     // (untransformed) column: its real part times the synthesis window.
@@ -887,9 +881,7 @@ FFT_CFFI_API int fftfree_execute_c2c(void* handle, const float* in, float* out, 
     a.polar_in = c->store_polar ? 1 : 0;
     a.inverse = c->inverse ? 1 : 0;
     a.pf = c->post_flags();
-    const int logr = choose_logr(ilog2((size_t)c->N), c->logr_req);
-    if (logr < 0) return 0;
-    FFB_CHECK(launch_c2c(a, logr, c->stream, &c->launches));
+    FFB_CHECK(launch_c2c(a, c->logr_req, c->stream, &c->launches));
     finish_out(c, o);
     finish_call(c, any_host);
     return 1;
@@ -941,7 +933,7 @@ FFT_CFFI_API int fftfree_ctx_schedule(void* handle, int* radices, int max_passes
   const int lg = ilog2((size_t)c->N);
   const bool real_in = c->eff_transform() == 1;  // batched STFT of real frames halves the size
   const int logm = real_in ? std::max(0, lg - 1) : lg;
-  const int logr = choose_logr(logm, c->logr_req);
+  const int logr = choose_logr(logm, c->logr_req, real_in);
   if (logr < 0) return 0;
   const int lr = std::min(logr, logm);
   int n = 0;

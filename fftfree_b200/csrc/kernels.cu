@@ -53,7 +53,25 @@ __device__ __forceinline__ float2 polar_to_complex(float2 u) {
 
 __device__ __forceinline__ bool aligned8(const void* p) { return (reinterpret_cast<uintptr_t>(p) & 7) == 0; }
 
+// Post-hook with the polar / magnitude choice fixed at compile time
+// (MODE 0: none or imag clear, 1: reduce_magnitude, 2: store_polar), so an
+// unrolled epilogue carries only the arithmetic it needs.
+template <int MODE>
+__device__ __forceinline__ float2 post_hook_m(float2 X, int k, int N, const PostFlags& pf) {
+  if (pf.r2c_half) {
+    if (k > (N >> 1)) X = make_float2(0.f, 0.f);
+    else if (k == 0 || k == (N >> 1)) X.y = 0.f;
+  }
+  if constexpr (MODE == 2) return make_float2(cabs_fast(X.x, X.y), atan2f(X.y, X.x));
+  if constexpr (MODE == 1) return make_float2(cabs_fast(X.x, X.y), 0.f);
+  if (pf.clear_imag) X.y = 0.f;
+  return X;
+}
+
+__host__ __device__ inline int post_mode(const PostFlags& pf) { return pf.polar ? 2 : (pf.reduce ? 1 : 0); }
+
 // ------------------------------------------------------------------ STFT IO
+template <int MODE>
 struct StftIO {
   StftArgs a;
   int logN;
@@ -111,43 +129,58 @@ struct StftIO {
     }
   }
 
+  // Bin k of the output: inverse scaling, exact-real DC / Nyquist, post
+  // hook, and the three planar stores (fft_cffi.cpp:813-824).
+  __device__ __forceinline__ void emit(float* re, float* im, float* mg, int k, float2 X, bool dc_or_nyq,
+                                       float inv_n, bool mag_is_re) const {
+    if (a.inverse) X = make_float2(X.x * inv_n, -X.y * inv_n);
+    // Real input: DC and Nyquist are exactly real (imag +0), as in the
+    // reference's radix-2 executors.
+    if (dc_or_nyq) X.y = 0.f;
+    X = post_hook_m<MODE>(X, k, a.N, a.pf);
+    re[k] = X.x;
+    im[k] = X.y;
+    mg[k] = mag_is_re ? X.x : cabs_fast(X.x, X.y);
+  }
+
   template <class S>
   __device__ __forceinline__ void store(long long f, int t, float2 (&v)[S::R], float2* sm,
                                         const Twiddles& tw) const {
-    constexpr int M = S::M;
+    constexpr int M = S::M, T = S::T, R = S::R;
     tile_write_natural<S>(v, t, sm);
     __syncthreads();
     if (f >= a.frames) return;
-    const int N = a.N;
     const long long ob = f * a.out_stride;
-    const float inv_n = 1.0f / (float)N;
-    const bool mag_is_re = a.pf.reduce || (a.pf.polar && a.mag_from_real);
-    for (int k = t; k < a.out_bins; k += S::T) {
-      int kk = k;
-      bool cj = false;
-      if (kk > (N >> 1)) { kk = N - kk; cj = true; }
-      float2 X;
-      if (N == 1) {
-        X = sm[0];
-      } else {
-        // Real-input untangle of the N/2-point transform Z of z[m] = x[2m] + i x[2m+1]:
-        // X[k] = E + w^k O,  E = (Z[k] + conj Z[M-k]) / 2,  O = -i (Z[k] - conj Z[M-k]) / 2
-        const float2 zk = sm[pidx(kk & (M - 1))];
-        const float2 zm = sm[pidx((M - kk) & (M - 1))];
-        const float2 E = make_float2(0.5f * (zk.x + zm.x), 0.5f * (zk.y - zm.y));
-        const float2 D = make_float2(zk.x - zm.x, zk.y + zm.y);
-        const float2 O = make_float2(0.5f * D.y, -0.5f * D.x);
-        X = cadd(E, cmul(tw_get(tw, logN, (unsigned)kk), O));
-      }
-      if (cj) X = cconj(X);
-      if (a.inverse) X = make_float2(X.x * inv_n, -X.y * inv_n);
-      // Real input: DC and Nyquist are exactly real (imag +0), as in the
-      // reference's radix-2 executors.
-      if (kk == 0 || 2 * kk == N) X.y = 0.f;
-      X = post_hook(X, k, N, a.pf);
-      a.out_re[ob + k] = X.x;
-      a.out_im[ob + k] = X.y;
-      a.out_mag[ob + k] = mag_is_re ? X.x : cabs_fast(X.x, X.y);
+    float* re = a.out_re + ob;
+    float* im = a.out_im + ob;
+    float* mg = a.out_mag + ob;
+    const bool mag_is_re = (MODE == 1) || (MODE == 2 && a.mag_from_real);
+    if (a.N == 1) {
+      if (t == 0) emit(re, im, mg, 0, make_float2(v[0].x, 0.f), true, 1.0f, mag_is_re);
+      return;
+    }
+    constexpr int LN = S::LOGM + 1;  // N = 2M
+    const float inv_n = 1.0f / (float)(2 * M);
+    const int bins = a.out_bins;
+    // Real-input untangle of the M-point transform Z of z[m] = x[2m] + i x[2m+1]:
+    // X[k] = E + w^k O,  E = (Z[k] + conj Z[M-k]) / 2,  O = -i (Z[k] - conj Z[M-k]) / 2.
+    // This thread holds Z[k] for k = t + i*T in v[i]; X[N-k] = conj X[k].
+    const float2* w = tw.pyr + ((1 << LN) - 1) + t;
+#pragma unroll
+    for (int i = 0; i < R; ++i) {
+      const int k = t + i * T;
+      const float2 zk = v[i];
+      const float2 zm = sm[pidx((M - k) & (M - 1))];
+      const float2 E = make_float2(0.5f * (zk.x + zm.x), 0.5f * (zk.y - zm.y));
+      const float2 D = make_float2(zk.x - zm.x, zk.y + zm.y);
+      const float2 O = make_float2(0.5f * D.y, -0.5f * D.x);
+      const float2 X = cadd(E, cmul(__ldg(w + i * T), O));
+      if (k < bins) emit(re, im, mg, k, X, k == 0, inv_n, mag_is_re);
+      if (k > 0 && 2 * M - k < bins) emit(re, im, mg, 2 * M - k, cconj(X), false, inv_n, mag_is_re);
+    }
+    if (t == 0 && M < bins) {
+      // Nyquist: X[M] = Re Z[0] - Im Z[0]
+      emit(re, im, mg, M, make_float2(v[0].x - v[0].y, 0.f), true, inv_n, mag_is_re);
     }
   }
 };
@@ -283,37 +316,50 @@ struct C2rHalfIO {
   CplxBatchArgs a;
   int logN;
 
+  // X[k] as the Hermitian rebuild sees it (fft_cffi.cpp:1073-1078, and the
+  // Cooley-Tukey pre-hook's polar conversion eigen_fft.hpp:2511-2522),
+  // conjugated for a forward context.
+  __device__ __forceinline__ float2 bin(const float* re, const float* im, int k, bool edge, float cs) const {
+    float2 u = make_float2(__ldg(re + k), __ldg(im + k));
+    if (edge) u.y = 0.f;
+    if (a.ct_pre == 2 && a.polar_in) {
+      u = polar_to_complex(u);
+      if (edge) u.y = 0.f;
+    }
+    u.y *= cs;
+    return u;
+  }
+
   template <class S>
   __device__ __forceinline__ void load(long long f, int t, float2 (&v)[S::R], float2* sm,
                                        const Twiddles& tw) const {
-    constexpr int M = S::M;
+    constexpr int M = S::M, T = S::T, R = S::R;
+    constexpr int LN = S::LOGM + 1;
     const bool ok = f < a.frames;
+    float2 xk[R];
     if (ok) {
       const float* re = a.in_re + f * (long long)a.bins;
       const float* im = a.in_im + f * (long long)a.bins;
       const float cs = a.inverse ? 1.f : -1.f;  // forward: conjugate spectrum
-      for (int k = t; k <= M; k += S::T) {
-        float2 u = make_float2(__ldg(re + k), __ldg(im + k));
-        if (k == 0 || k == M) u.y = 0.f;  // fft_cffi.cpp:1073-1078
-        if (a.ct_pre == 2 && a.polar_in) {  // eigen_fft.hpp:2511-2522
-          u = polar_to_complex(u);
-          if (k == 0 || k == M) u.y = 0.f;
-        }
-        u.y *= cs;
-        sm[pidx(k)] = u;
+#pragma unroll
+      for (int i = 0; i < R; ++i) {
+        const int k = t + i * T;
+        xk[i] = bin(re, im, k, k == 0, cs);
+        sm[pidx(k)] = xk[i];
       }
+      if (t == 0) sm[pidx(M)] = bin(re, im, M, true, cs);
     }
     __syncthreads();
+    const float2* w = tw.pyr + ((1 << LN) - 1) + t;
 #pragma unroll
-    for (int i = 0; i < S::R; ++i) {
-      const int m = t + i * S::T;
+    for (int i = 0; i < R; ++i) {
+      const int m = t + i * T;
       float2 z = make_float2(0.f, 0.f);
       if (ok) {
-        const float2 xk = sm[pidx(m)];
         const float2 xm = sm[pidx(M - m)];
-        const float2 E = make_float2(0.5f * (xk.x + xm.x), 0.5f * (xk.y - xm.y));
-        const float2 D = make_float2(0.5f * (xk.x - xm.x), 0.5f * (xk.y + xm.y));
-        const float2 O = cmul(D, cconj(tw_get(tw, logN, (unsigned)m)));
+        const float2 E = make_float2(0.5f * (xk[i].x + xm.x), 0.5f * (xk[i].y - xm.y));
+        const float2 D = make_float2(0.5f * (xk[i].x - xm.x), 0.5f * (xk[i].y + xm.y));
+        const float2 O = cmul(D, cconj(__ldg(w + i * T)));
         z = make_float2(E.x - O.y, E.y + O.x);  // E + i O
       }
       v[i] = cconj(z);  // IDFT via conj . DFT . conj
@@ -433,12 +479,16 @@ static cudaError_t dispatch(const IO& io, int logm, int logr, long long n, cudaS
 
 int max_single_pass_log() { return 13; }
 
-int choose_logr(int logm, int requested_log) {
+int choose_logr(int logm, int requested_log, bool real_path) {
   if (logm > max_single_pass_log()) return -1;
   auto valid = [&](int lr) { return lr >= 2 && lr <= 4 && (logm - (lr < logm ? lr : logm)) <= 10; };
   if (requested_log >= 2 && requested_log <= 4 && valid(requested_log)) return requested_log;
-  // default schedule: radix 16 for large transforms, 8 for mid, 4 for small
-  int lr = (logm >= 10) ? 4 : (logm >= 6 ? 3 : 2);
+  // Default schedule, from B200 sweeps: complex transforms radix 16 from
+  // 1024 points up, 8 below; the real-input paths (which add an untangle
+  // step per bin) radix 8 up to 4096 points.
+  int lr;
+  if (real_path) lr = (logm >= 13) ? 4 : (logm >= 6 ? 3 : 2);
+  else lr = (logm >= 10) ? 4 : (logm >= 6 ? 3 : 2);
   while (!valid(lr) && lr < 4) ++lr;
   return valid(lr) ? lr : -1;
 }
@@ -449,24 +499,36 @@ static int ilog2i(long long n) {
   return l;
 }
 
-cudaError_t launch_stft(const StftArgs& a, int logr, cudaStream_t s, uint64_t* launches) {
-  StftIO io{a, ilog2i(a.N)};
+cudaError_t launch_stft(const StftArgs& a, int req_logr, cudaStream_t s, uint64_t* launches) {
   const int logm = (a.N == 1) ? 0 : ilog2i(a.N) - 1;
-  return dispatch(io, logm, logr, a.frames, s, launches);
+  const int logr = choose_logr(logm, req_logr, true);
+  if (logr < 0) return cudaErrorInvalidValue;
+  switch (post_mode(a.pf)) {
+    case 2: return dispatch(StftIO<2>{a, ilog2i(a.N)}, logm, logr, a.frames, s, launches);
+    case 1: return dispatch(StftIO<1>{a, ilog2i(a.N)}, logm, logr, a.frames, s, launches);
+    default: return dispatch(StftIO<0>{a, ilog2i(a.N)}, logm, logr, a.frames, s, launches);
+  }
 }
 
-cudaError_t launch_c2c(const C2cArgs& a, int logr, cudaStream_t s, uint64_t* launches) {
+cudaError_t launch_c2c(const C2cArgs& a, int req_logr, cudaStream_t s, uint64_t* launches) {
   C2cIO io{a};
-  return dispatch(io, ilog2i(a.N), logr, a.batch, s, launches);
+  const int logm = ilog2i(a.N);
+  const int logr = choose_logr(logm, req_logr, false);
+  if (logr < 0) return cudaErrorInvalidValue;
+  return dispatch(io, logm, logr, a.batch, s, launches);
 }
 
-cudaError_t launch_cplx_batch(const CplxBatchArgs& a, int logr, cudaStream_t s, uint64_t* launches) {
+cudaError_t launch_cplx_batch(const CplxBatchArgs& a, int req_logr, cudaStream_t s, uint64_t* launches) {
   const int lg = ilog2i(a.N);
   if (a.c2r_half && a.N >= 4) {
     C2rHalfIO io{a, lg};
+    const int logr = choose_logr(lg - 1, req_logr, true);
+    if (logr < 0) return cudaErrorInvalidValue;
     return dispatch(io, lg - 1, logr, a.frames, s, launches);
   }
   CplxBatchIO io{a};
+  const int logr = choose_logr(lg, req_logr, false);
+  if (logr < 0) return cudaErrorInvalidValue;
   return dispatch(io, lg, logr, a.frames, s, launches);
 }
 

@@ -76,12 +76,14 @@ const float2* twiddle_pyramid(int max_log, cudaStream_t stream);
 const float2* twiddle_pass_tables(cudaStream_t stream);
 
 // Pick the single-pass radix (log2) for a transform of 2^logm points;
-// `requested_log` (2..4) is honoured when valid.  Returns -1 if the size
-// needs the multi-pass path.
-int choose_logr(int logm, int requested_log);
+// `requested_log` (2..4) is honoured when valid, otherwise the tuned
+// default for complex (`real_path` false) or real-input paths applies.
+// Returns -1 if the size needs the multi-pass path.
+int choose_logr(int logm, int requested_log, bool real_path);
 int max_single_pass_log();
 
-// Launchers return cudaSuccess or the launch error.  `launches` is
+// Launchers return cudaSuccess or the launch error.  `req_logr` is the
+// context's requested pass radix (log2, -1 = default).  `launches` is
 // incremented by the number of kernels enqueued.
 cudaError_t launch_stft(const StftArgs& a, int logr, cudaStream_t s, uint64_t* launches);
 cudaError_t launch_c2c(const C2cArgs& a, int logr, cudaStream_t s, uint64_t* launches);

@@ -98,8 +98,7 @@ extern "C" FFT_CFFI_API size_t fftfree_execute_complex_batched_noalloc(void* han
                            "memory (host buffers would need staging allocations)\n");
       break;
     }
-    const int logr = choose_logr(ilog2i(N), c->logr_req);
-    if (logr < 0) {
+    if (ilog2i(N) > max_single_pass_log()) {
       std::fprintf(stderr, "[fftfree_b200] fftfree_execute_complex_batched_noalloc: N=%d not supported\n", N);
       break;
     }
@@ -125,7 +124,7 @@ extern "C" FFT_CFFI_API size_t fftfree_execute_complex_batched_noalloc(void* han
     a.out = frames_buf;
     // The transform writes every one of the frames * N scratch samples before
     // the overlap-add reads them, so nothing has to be cleared between calls.
-    if (launch_cplx_batch(a, logr, c->stream, &c->launches) != cudaSuccess) break;
+    if (launch_cplx_batch(a, c->logr_req, c->stream, &c->launches) != cudaSuccess) break;
     if (c->apply_ola) {
       OlaArgs o{};
       o.frames_buf = frames_buf;
