@@ -162,6 +162,37 @@ struct StftIO {
     constexpr int LN = S::LOGM + 1;  // N = 2M
     const float inv_n = 1.0f / (float)(2 * M);
     const int bins = a.out_bins;
+    if (bins == M + 1 && !a.inverse) {
+      // Common STFT case (half spectrum, forward): bins 0..M, each written
+      // once, no bounds or mirror logic.
+      const float2* w = tw.pyr + ((1 << LN) - 1) + t;
+      float* pr = re + t;
+      float* pi = im + t;
+      float* pm = mg + t;
+#pragma unroll
+      for (int i = 0; i < R; ++i) {
+        const float2 zk = v[i];
+        const float2 zm = sm[pidx((M - t - i * T) & (M - 1))];
+        const float2 E = make_float2(0.5f * (zk.x + zm.x), 0.5f * (zk.y - zm.y));
+        const float2 D = make_float2(zk.x - zm.x, zk.y + zm.y);
+        const float2 O = make_float2(0.5f * D.y, -0.5f * D.x);
+        float2 X = cadd(E, cmul(__ldg(w + i * T), O));
+        if (i == 0 && t == 0) X.y = 0.f;  // DC
+        float mag;
+        if constexpr (MODE == 2) { mag = cabs_fast(X.x, X.y); X = make_float2(mag, atan2f(X.y, X.x)); }
+        else if constexpr (MODE == 1) { mag = cabs_fast(X.x, X.y); X = make_float2(mag, 0.f); }
+        else {
+          if (a.pf.clear_imag) X.y = 0.f;
+          mag = cabs_fast(X.x, X.y);
+        }
+        if constexpr (MODE == 2) mag = a.mag_from_real ? X.x : cabs_fast(X.x, X.y);
+        pr[i * T] = X.x;
+        pi[i * T] = X.y;
+        pm[i * T] = mag;
+      }
+      if (t == 0) emit(re, im, mg, M, make_float2(v[0].x - v[0].y, 0.f), true, inv_n, mag_is_re);
+      return;
+    }
     // Real-input untangle of the M-point transform Z of z[m] = x[2m] + i x[2m+1]:
     // X[k] = E + w^k O,  E = (Z[k] + conj Z[M-k]) / 2,  O = -i (Z[k] - conj Z[M-k]) / 2.
     // This thread holds Z[k] for k = t + i*T in v[i]; X[N-k] = conj X[k].
