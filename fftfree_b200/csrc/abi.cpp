@@ -251,11 +251,23 @@ static int requested_logr(const FftContext* c) {
   return lg(c->radix);
 }
 
-// Transform sizes the single-pass kernels cover.
+// Transform sizes the kernels cover (single pass up to 2^13 complex points,
+// multi-pass beyond, up to 2^20).
 static bool size_supported(int N, bool real_input) {
+  (void)real_input;
+  return ilog2((size_t)N) <= max_multi_pass_log();
+}
+
+static bool single_pass(int N, bool real_input) {
   const int lg = ilog2((size_t)N);
   const int logm = real_input ? std::max(0, lg - 1) : lg;
   return logm <= max_single_pass_log();
+}
+
+static float2* scratch_for(FftContext* c, int N, long long batch, size_t* chunk) {
+  *chunk = four_step_chunk(ilog2((size_t)N), batch);
+  // two slots: the multi-pass pipeline alternates between them
+  return static_cast<float2*>(c->d_scratch.get(2 * *chunk * (size_t)N * sizeof(float2)));
 }
 
 static void setup_device(FftContext* c) {
@@ -328,7 +340,13 @@ static void run_stft(FftContext* c, const float* pcm, size_t pcm_len, size_t fra
   a.out_re = o_re.dev;
   a.out_im = o_im.dev;
   a.out_mag = o_mag.dev;
-  FFB_CHECK(launch_stft(a, c->logr_req, c->stream, &c->launches));
+  if (single_pass(c->N, true)) {
+    FFB_CHECK(launch_stft(a, c->logr_req, c->stream, &c->launches));
+  } else {
+    size_t chunk = 0;
+    float2* scratch = scratch_for(c, c->N, (long long)frames, &chunk);
+    FFB_CHECK(launch_four_step_stft(a, scratch, chunk, c->stream, &c->launches));
+  }
   finish_out(c, o_re);
   finish_out(c, o_im);
   finish_out(c, o_mag);
@@ -367,7 +385,13 @@ static void run_complex_batch(FftContext* c, const float* in_re, const float* in
   a.synth = c->windows_enabled ? static_cast<const float*>(c->d_synthesis.p) : nullptr;
   float* frames_out = c->apply_ola ? static_cast<float*>(c->d_frames.get(outn * sizeof(float))) : o.dev;
   a.out = frames_out;
-  FFB_CHECK(launch_cplx_batch(a, c->logr_req, c->stream, &c->launches));
+  if (single_pass(N, a.c2r_half && N >= 4)) {
+    FFB_CHECK(launch_cplx_batch(a, c->logr_req, c->stream, &c->launches));
+  } else {
+    size_t chunk = 0;
+    float2* scratch = scratch_for(c, N, (long long)frames, &chunk);
+    FFB_CHECK(launch_four_step_cplx(a, scratch, chunk, c->stream, &c->launches));
+  }
   if (raw_frames) {
     // Frames the recovery coordinator gave up on keep the restored
     // (untransformed) column: its real part times the synthesis window.
@@ -626,6 +650,7 @@ FFT_CFFI_API void fft_free(void* handle) {
     c->d_out2.release();
     c->d_frames.release();
     c->d_meta_tw.release();
+    c->d_scratch.release();
     c->magic = 0;
   }
   delete c;
@@ -881,7 +906,13 @@ FFT_CFFI_API int fftfree_execute_c2c(void* handle, const float* in, float* out, 
     a.polar_in = c->store_polar ? 1 : 0;
     a.inverse = c->inverse ? 1 : 0;
     a.pf = c->post_flags();
-    FFB_CHECK(launch_c2c(a, c->logr_req, c->stream, &c->launches));
+    if (single_pass(c->N, false)) {
+      FFB_CHECK(launch_c2c(a, c->logr_req, c->stream, &c->launches));
+    } else {
+      size_t chunk = 0;
+      float2* scratch = scratch_for(c, c->N, (long long)batch, &chunk);
+      FFB_CHECK(launch_four_step_c2c(a, scratch, chunk, c->stream, &c->launches));
+    }
     finish_out(c, o);
     finish_call(c, any_host);
     return 1;

@@ -69,6 +69,7 @@ struct FftContext {
   bool windows_uploaded = false;
   DevBuf d_in0, d_in1, d_out0, d_out1, d_out2, d_frames;
   DevBuf d_meta_tw;  // reference float twiddle table for the metadata path
+  DevBuf d_scratch;  // multi-pass intermediate chunk
   uint64_t launches = 0;
   std::recursive_mutex mu;
 

@@ -1,16 +1,16 @@
-// kernels.cu -- single-pass batched FFT kernels for sm_100a and their
-// launchers: real-frame STFT (fused framing, window, zero-pad, mirror, R2C
-// half-size untangle, hooks, planar epilogue), complex C2C with the plan's
-// hooks, complex/inverse batch, and the overlap-add gather.
-#include "kernels.h"
-#include "fft_engine.cuh"
+// io.cuh -- per-path load/store policies of the FFT kernels (device code):
+// STFT framing + real-input untangle epilogue, complex C2C with the plan's
+// hooks, complex/inverse batch, Hermitian C2R half-size path.  Each policy
+// also provides elem4/emit4 (one input element / one output bin by index)
+// for the multi-pass kernels.
+#pragma once
 
-#include <cmath>
-#include <mutex>
-#include <vector>
+#include <stdint.h>
+
+#include "fft_engine.cuh"
+#include "kernels.h"
 
 namespace ffb {
-
 // ------------------------------------------------------------------ hooks
 // |z| as sqrt(x^2 + y^2): the squares summed with one rounding (fma), then
 // the correctly rounded square root; magnitudes whose squares could
@@ -129,6 +129,28 @@ struct StftIO {
     }
   }
 
+  // Multi-pass access: input element n of frame f as a complex value (the
+  // frame is real), and output bin k of the N-point transform.
+  __device__ __forceinline__ float2 elem4(long long f, long long n) const {
+    if (f >= a.frames) return make_float2(0.f, 0.f);
+    int nn = (int)n;
+    if (a.mirror && nn > (a.N >> 1)) nn = a.N - nn;
+    const long long start = f * (long long)a.H;
+    long long cnt = a.pcm_len - start;
+    if (cnt > a.W) cnt = a.W;
+    if ((long long)nn >= cnt) return make_float2(0.f, 0.f);
+    float s = __ldg(a.pcm + start + nn);
+    if (a.win) s *= __ldg(a.win + nn);
+    return make_float2(s, 0.f);
+  }
+  __device__ __forceinline__ void emit4(long long f, long long k, float2 X) const {
+    if (f >= a.frames || k >= a.out_bins) return;
+    const long long ob = f * a.out_stride;
+    const bool mag_is_re = (MODE == 1) || (MODE == 2 && a.mag_from_real);
+    emit(a.out_re + ob, a.out_im + ob, a.out_mag + ob, (int)k, X, k == 0 || 2 * k == a.N,
+         1.0f / (float)a.N, mag_is_re);
+  }
+
   // Bin k of the output: inverse scaling, exact-real DC / Nyquist, post
   // hook, and the three planar stores (fft_cffi.cpp:813-824).
   __device__ __forceinline__ void emit(float* re, float* im, float* mg, int k, float2 X, bool dc_or_nyq,
@@ -238,6 +260,17 @@ struct C2cIO {
     return col[n];
   }
 
+  __device__ __forceinline__ float2 elem4(long long b, long long n) const {
+    if (b >= a.batch) return make_float2(0.f, 0.f);
+    const float2 u = elem(a.in + b * (long long)a.N, (int)n);
+    return a.inverse ? cconj(u) : u;
+  }
+  __device__ __forceinline__ void emit4(long long b, long long k, float2 X) const {
+    if (b >= a.batch) return;
+    if (a.inverse) X = cscale(cconj(X), 1.0f / (float)a.N);
+    a.out[b * (long long)a.N + k] = post_hook(X, (int)k, a.N, a.pf);
+  }
+
   template <class S>
   __device__ __forceinline__ void load(long long b, int t, float2 (&v)[S::R], float2*, const Twiddles&) const {
     if (b >= a.batch) {
@@ -305,6 +338,20 @@ struct CplxBatchIO {
     float2 u = base(f, n);
     if (a.ct_pre == 1) u.y = 0.f;
     return u;
+  }
+
+  __device__ __forceinline__ float2 elem4(long long f, long long n) const {
+    if (f >= a.frames) return make_float2(0.f, 0.f);
+    const float2 u = elem(f, (int)n);
+    return a.inverse ? cconj(u) : u;
+  }
+  __device__ __forceinline__ void emit4(long long f, long long k, float2 X) const {
+    if (f >= a.frames) return;
+    if (a.inverse) X = cscale(cconj(X), 1.0f / (float)a.N);
+    X = post_hook(X, (int)k, a.N, a.pf);
+    float s = X.x;
+    if (a.synth) s *= __ldg(a.synth + k);
+    a.out[f * (long long)a.N + k] = s;
   }
 
   template <class S>
@@ -424,300 +471,5 @@ struct C2rHalfIO {
     }
   }
 };
-
-// ------------------------------------------------------------------ kernel
-template <class S>
-struct Launch {
-  static constexpr int G = (S::T >= 256) ? 1 : 256 / S::T;  // transforms per block
-  static constexpr int BLOCK = S::T * G;
-};
-
-template <class S, class IO>
-__global__ void __launch_bounds__(Launch<S>::BLOCK)
-k_fft(IO io, Twiddles tw) {
-  extern __shared__ float2 smem[];
-  constexpr int T = S::T;
-  const int g = threadIdx.x / T;
-  const int t = threadIdx.x - g * T;
-  const long long b = (long long)blockIdx.x * Launch<S>::G + g;
-  float2* sm = smem + g * S::SMEM;
-  float2 v[S::R];
-  io.template load<S>(b, t, v, sm, tw);
-  fft_engine<S>(v, t, sm, tw);
-  io.template store<S>(b, t, v, sm, tw);
-}
-
-template <class S, class IO>
-static cudaError_t run(const IO& io, long long nbatch, cudaStream_t st, uint64_t* launches) {
-  using L = Launch<S>;
-  if (nbatch <= 0) return cudaSuccess;
-  const long long grid = (nbatch + L::G - 1) / L::G;
-  if (grid > 0x7fffffffLL) return cudaErrorInvalidValue;
-  const size_t smem = (size_t)L::G * S::SMEM * sizeof(float2);
-  if (smem > 48 * 1024) {
-    cudaError_t e = cudaFuncSetAttribute(k_fft<S, IO>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         (int)smem);
-    if (e != cudaSuccess) return e;
-  }
-  Twiddles tw{twiddle_pyramid(0, st), twiddle_pass_tables(st)};
-  k_fft<S, IO><<<(unsigned)grid, L::BLOCK, smem, st>>>(io, tw);
-  if (launches) ++*launches;
-  return cudaGetLastError();
-}
-
-// Compile-time table of instantiations: LOGM 0..13, LOGR 2..4 (clamped by
-// Sched), threads per transform <= 1024.
-template <class IO, int LOGM, int LOGR>
-static cudaError_t run_if_valid(const IO& io, long long n, cudaStream_t st, uint64_t* l) {
-  using S = Sched<LOGM, LOGR>;
-  if constexpr (S::T > 1024) {
-    return cudaErrorInvalidValue;
-  } else {
-    return run<S, IO>(io, n, st, l);
-  }
-}
-
-template <class IO, int LOGM>
-static cudaError_t dispatch_r(const IO& io, int logr, long long n, cudaStream_t st, uint64_t* l) {
-  switch (logr) {
-    case 2: return run_if_valid<IO, LOGM, 2>(io, n, st, l);
-    case 3: return run_if_valid<IO, LOGM, 3>(io, n, st, l);
-    default: return run_if_valid<IO, LOGM, 4>(io, n, st, l);
-  }
-}
-
-template <class IO>
-static cudaError_t dispatch(const IO& io, int logm, int logr, long long n, cudaStream_t st,
-                            uint64_t* l) {
-  switch (logm) {
-    case 0: return dispatch_r<IO, 0>(io, logr, n, st, l);
-    case 1: return dispatch_r<IO, 1>(io, logr, n, st, l);
-    case 2: return dispatch_r<IO, 2>(io, logr, n, st, l);
-    case 3: return dispatch_r<IO, 3>(io, logr, n, st, l);
-    case 4: return dispatch_r<IO, 4>(io, logr, n, st, l);
-    case 5: return dispatch_r<IO, 5>(io, logr, n, st, l);
-    case 6: return dispatch_r<IO, 6>(io, logr, n, st, l);
-    case 7: return dispatch_r<IO, 7>(io, logr, n, st, l);
-    case 8: return dispatch_r<IO, 8>(io, logr, n, st, l);
-    case 9: return dispatch_r<IO, 9>(io, logr, n, st, l);
-    case 10: return dispatch_r<IO, 10>(io, logr, n, st, l);
-    case 11: return dispatch_r<IO, 11>(io, logr, n, st, l);
-    case 12: return dispatch_r<IO, 12>(io, logr, n, st, l);
-    case 13: return dispatch_r<IO, 13>(io, logr, n, st, l);
-    default: return cudaErrorInvalidValue;
-  }
-}
-
-int max_single_pass_log() { return 13; }
-
-int choose_logr(int logm, int requested_log, bool real_path) {
-  if (logm > max_single_pass_log()) return -1;
-  auto valid = [&](int lr) { return lr >= 2 && lr <= 4 && (logm - (lr < logm ? lr : logm)) <= 10; };
-  if (requested_log >= 2 && requested_log <= 4 && valid(requested_log)) return requested_log;
-  // Default schedule, from B200 sweeps: complex transforms radix 16 from
-  // 1024 points up, 8 below; the real-input paths (which add an untangle
-  // step per bin) radix 8 up to 4096 points.
-  int lr;
-  if (real_path) lr = (logm >= 13) ? 4 : (logm >= 6 ? 3 : 2);
-  else lr = (logm >= 10) ? 4 : (logm >= 6 ? 3 : 2);
-  while (!valid(lr) && lr < 4) ++lr;
-  return valid(lr) ? lr : -1;
-}
-
-static int ilog2i(long long n) {
-  int l = 0;
-  while ((1LL << l) < n) ++l;
-  return l;
-}
-
-cudaError_t launch_stft(const StftArgs& a, int req_logr, cudaStream_t s, uint64_t* launches) {
-  const int logm = (a.N == 1) ? 0 : ilog2i(a.N) - 1;
-  const int logr = choose_logr(logm, req_logr, true);
-  if (logr < 0) return cudaErrorInvalidValue;
-  switch (post_mode(a.pf)) {
-    case 2: return dispatch(StftIO<2>{a, ilog2i(a.N)}, logm, logr, a.frames, s, launches);
-    case 1: return dispatch(StftIO<1>{a, ilog2i(a.N)}, logm, logr, a.frames, s, launches);
-    default: return dispatch(StftIO<0>{a, ilog2i(a.N)}, logm, logr, a.frames, s, launches);
-  }
-}
-
-cudaError_t launch_c2c(const C2cArgs& a, int req_logr, cudaStream_t s, uint64_t* launches) {
-  C2cIO io{a};
-  const int logm = ilog2i(a.N);
-  const int logr = choose_logr(logm, req_logr, false);
-  if (logr < 0) return cudaErrorInvalidValue;
-  return dispatch(io, logm, logr, a.batch, s, launches);
-}
-
-cudaError_t launch_cplx_batch(const CplxBatchArgs& a, int req_logr, cudaStream_t s, uint64_t* launches) {
-  const int lg = ilog2i(a.N);
-  if (a.c2r_half && a.N >= 4) {
-    C2rHalfIO io{a, lg};
-    const int logr = choose_logr(lg - 1, req_logr, true);
-    if (logr < 0) return cudaErrorInvalidValue;
-    return dispatch(io, lg - 1, logr, a.frames, s, launches);
-  }
-  CplxBatchIO io{a};
-  const int logr = choose_logr(lg, req_logr, false);
-  if (logr < 0) return cudaErrorInvalidValue;
-  return dispatch(io, lg, logr, a.frames, s, launches);
-}
-
-// ------------------------------------------------------------------ OLA
-// fft_cffi.cpp:1119-1146: out[t] = sum over frames f with f*H <= t < f*H + N
-// of frame_f[t - f*H], t < frames*N, accumulated in frame order; with COLA,
-// divided by the summed weights where that sum exceeds 1e-12.
-__global__ void k_ola(OlaArgs a) {
-  const long long total = a.frames * (long long)a.N;
-  for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < total;
-       t += (long long)gridDim.x * blockDim.x) {
-    long long fhi = t / a.H;
-    if (fhi > a.frames - 1) fhi = a.frames - 1;
-    const long long flo = (t >= a.N) ? (t - a.N) / a.H + 1 : 0;
-    float acc = 0.f, nrm = 0.f;
-    for (long long f = flo; f <= fhi; ++f) {
-      const long long i = t - f * a.H;
-      acc += __ldg(a.frames_buf + f * a.N + i);
-      if (a.cola) nrm += a.weight ? __ldg(a.weight + i) : 1.0f;
-    }
-    if (a.cola && nrm > 1e-12f) acc /= nrm;
-    a.out[t] = acc;
-  }
-}
-
-cudaError_t launch_ola(const OlaArgs& a, cudaStream_t s, uint64_t* launches) {
-  const long long total = a.frames * (long long)a.N;
-  if (total <= 0) return cudaSuccess;
-  long long blocks = (total + 255) / 256;
-  if (blocks > 148 * 64) blocks = 148 * 64;
-  k_ola<<<(unsigned)blocks, 256, 0, s>>>(a);
-  if (launches) ++*launches;
-  return cudaGetLastError();
-}
-
-// ------------------------------------------------------------------ twiddles
-namespace {
-struct Pyramid {
-  int max_log = -1;
-  float2* dev = nullptr;
-};
-std::mutex g_tw_mu;
-std::vector<Pyramid> g_tw;  // per device
-}  // namespace
-
-// exp(-2 pi i e / 2^L) in FP64 from the first octant with exact symmetry:
-// quarter points are exactly 0 / +-1 and mirrored entries share bits.
-static void octant_value(long long e, int L, double* c, double* s) {
-  const long long n = 1LL << L;
-  e &= (n - 1);
-  if (L < 3) {
-    // n in {1, 2, 4}: exact table
-    static const double cs[4][2] = {{1, 0}, {0, -1}, {-1, 0}, {0, 1}};
-    const long long q = (n == 1) ? 0 : e * (4 / n);
-    *c = cs[q][0];
-    *s = cs[q][1];
-    return;
-  }
-  const long long n8 = n >> 3;
-  const long long oct = e / n8;
-  const long long r = e - oct * n8;
-  // angle theta = 2 pi e / n = (pi/4) * oct + phi, phi = 2 pi r / n in [0, pi/4)
-  auto base = [&](long long rr, double* cc, double* ss) {
-    const double phi = 2.0 * M_PI * (double)rr / (double)n;
-    *cc = std::cos(phi);
-    *ss = std::sin(phi);
-  };
-  double cr, sr, cq, sq;
-  base(r, &cr, &sr);          // cos/sin(phi)
-  base(n8 - r, &cq, &sq);     // cos/sin(pi/4 - phi)
-  double C, S;                // cos/sin(theta)
-  switch (oct) {
-    case 0: C = cr; S = sr; break;
-    case 1: C = sq; S = cq; break;        // theta = pi/2 - (pi/4 - phi)
-    case 2: C = -sr; S = cr; break;       // theta = pi/2 + phi
-    case 3: C = -cq; S = sq; break;       // theta = pi - (pi/4 - phi)
-    case 4: C = -cr; S = -sr; break;      // theta = pi + phi
-    case 5: C = -sq; S = -cq; break;
-    case 6: C = sr; S = -cr; break;       // theta = 3pi/2 + phi
-    default: C = cq; S = -sq; break;      // theta = 2pi - (pi/4 - phi)
-  }
-  if (r == 0) {  // exact octant points
-    const double h = std::sqrt(0.5);
-    static const double ex[8][2] = {{1, 0}, {0, 0}, {0, 1}, {0, 0}, {-1, 0}, {0, 0}, {0, -1}, {0, 0}};
-    if ((oct & 1) == 0) { C = ex[oct][0]; S = ex[oct][1]; }
-    else {
-      C = (oct == 1 || oct == 7) ? h : -h;
-      S = (oct == 1 || oct == 3) ? h : -h;
-    }
-  }
-  *c = C;
-  *s = (S == 0.0) ? 0.0 : -S;  // exp(-i theta), without negative zeros
-}
-
-const float2* twiddle_pyramid(int max_log, cudaStream_t stream) {
-  int dev = 0;
-  cudaGetDevice(&dev);
-  std::lock_guard<std::mutex> lk(g_tw_mu);
-  if ((int)g_tw.size() <= dev) g_tw.resize(dev + 1);
-  Pyramid& p = g_tw[dev];
-  const int want = max_log < 18 ? 18 : max_log;
-  if (p.dev && p.max_log >= want) return p.dev;
-  const size_t total = ((size_t)1 << (want + 1)) - 1;
-  std::vector<float2> host(total);
-  for (int L = 0; L <= want; ++L) {
-    const size_t off = ((size_t)1 << L) - 1;
-    for (long long e = 0; e < (1LL << L); ++e) {
-      double c, s;
-      octant_value(e, L, &c, &s);
-      host[off + e] = make_float2((float)c, (float)s);
-    }
-  }
-  float2* d = nullptr;
-  if (cudaMalloc(&d, total * sizeof(float2)) != cudaSuccess) return p.dev;
-  cudaMemcpyAsync(d, host.data(), total * sizeof(float2), cudaMemcpyHostToDevice, stream);
-  cudaStreamSynchronize(stream);
-  // The previous (smaller) table stays allocated: kernels still queued on
-  // other streams may read it.
-  p.dev = d;
-  p.max_log = want;
-  return p.dev;
-}
-
-
-namespace {
-std::vector<float2*> g_pass;  // per device, guarded by g_tw_mu
-}
-
-// Per-pass twiddle tables (layout in fft_engine.cuh, pass_table_offset):
-// w[(r-1)*Ns + k] = exp(-2 pi i k r / (Ns R)), built in FP64 with the same
-// octant symmetry as the pyramid.
-const float2* twiddle_pass_tables(cudaStream_t stream) {
-  int dev = 0;
-  cudaGetDevice(&dev);
-  std::lock_guard<std::mutex> lk(g_tw_mu);
-  if ((int)g_pass.size() <= dev) g_pass.resize(dev + 1, nullptr);
-  if (g_pass[dev]) return g_pass[dev];
-  const long long total = pass_table_size();
-  std::vector<float2> host((size_t)total);
-  for (int lr = 1; lr <= 4; ++lr) {
-    const int R = 1 << lr;
-    for (int lns = 0; lns <= kPassMaxLog; ++lns) {
-      const long long Ns = 1LL << lns;
-      const long long off = pass_table_offset(lr, lns);
-      for (int r = 1; r < R; ++r)
-        for (long long k = 0; k < Ns; ++k) {
-          double c, s;
-          octant_value(k * r, lns + lr, &c, &s);
-          host[(size_t)(off + (r - 1) * Ns + k)] = make_float2((float)c, (float)s);
-        }
-    }
-  }
-  float2* d = nullptr;
-  if (cudaMalloc(&d, host.size() * sizeof(float2)) != cudaSuccess) return nullptr;
-  cudaMemcpyAsync(d, host.data(), host.size() * sizeof(float2), cudaMemcpyHostToDevice, stream);
-  cudaStreamSynchronize(stream);
-  g_pass[dev] = d;
-  return d;
-}
 
 }  // namespace ffb

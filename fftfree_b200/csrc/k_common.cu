@@ -1,0 +1,183 @@
+// k_common.cu -- schedule choice, overlap-add gather and the twiddle tables.
+#include <cmath>
+#include <mutex>
+#include <vector>
+
+#include "fft_launch.cuh"
+
+namespace ffb {
+
+int max_single_pass_log() { return 13; }
+
+int choose_logr(int logm, int requested_log, bool real_path) {
+  if (logm > max_single_pass_log()) return -1;
+  auto valid = [&](int lr) { return lr >= 2 && lr <= 4 && (logm - (lr < logm ? lr : logm)) <= 10; };
+  if (requested_log >= 2 && requested_log <= 4 && valid(requested_log)) return requested_log;
+  // Default schedule, from B200 sweeps: complex transforms radix 16 from
+  // 1024 points up, 8 below; the real-input paths (which add an untangle
+  // step per bin) radix 8 up to 4096 points.
+  int lr;
+  if (real_path) lr = (logm >= 13) ? 4 : (logm >= 6 ? 3 : 2);
+  else lr = (logm >= 10) ? 4 : (logm >= 6 ? 3 : 2);
+  while (!valid(lr) && lr < 4) ++lr;
+  return valid(lr) ? lr : -1;
+}
+
+// ------------------------------------------------------------------ OLA
+// fft_cffi.cpp:1119-1146: out[t] = sum over frames f with f*H <= t < f*H + N
+// of frame_f[t - f*H], t < frames*N, accumulated in frame order; with COLA,
+// divided by the summed weights where that sum exceeds 1e-12.
+__global__ void k_ola(OlaArgs a) {
+  const long long total = a.frames * (long long)a.N;
+  for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < total;
+       t += (long long)gridDim.x * blockDim.x) {
+    long long fhi = t / a.H;
+    if (fhi > a.frames - 1) fhi = a.frames - 1;
+    const long long flo = (t >= a.N) ? (t - a.N) / a.H + 1 : 0;
+    float acc = 0.f, nrm = 0.f;
+    for (long long f = flo; f <= fhi; ++f) {
+      const long long i = t - f * a.H;
+      acc += __ldg(a.frames_buf + f * a.N + i);
+      if (a.cola) nrm += a.weight ? __ldg(a.weight + i) : 1.0f;
+    }
+    if (a.cola && nrm > 1e-12f) acc /= nrm;
+    a.out[t] = acc;
+  }
+}
+
+cudaError_t launch_ola(const OlaArgs& a, cudaStream_t s, uint64_t* launches) {
+  const long long total = a.frames * (long long)a.N;
+  if (total <= 0) return cudaSuccess;
+  long long blocks = (total + 255) / 256;
+  if (blocks > 148 * 64) blocks = 148 * 64;
+  k_ola<<<(unsigned)blocks, 256, 0, s>>>(a);
+  if (launches) ++*launches;
+  return cudaGetLastError();
+}
+
+// ------------------------------------------------------------------ twiddles
+namespace {
+struct Pyramid {
+  int max_log = -1;
+  float2* dev = nullptr;
+};
+std::mutex g_tw_mu;
+std::vector<Pyramid> g_tw;  // per device
+}  // namespace
+
+// exp(-2 pi i e / 2^L) in FP64 from the first octant with exact symmetry:
+// quarter points are exactly 0 / +-1 and mirrored entries share bits.
+static void octant_value(long long e, int L, double* c, double* s) {
+  const long long n = 1LL << L;
+  e &= (n - 1);
+  if (L < 3) {
+    // n in {1, 2, 4}: exact table
+    static const double cs[4][2] = {{1, 0}, {0, -1}, {-1, 0}, {0, 1}};
+    const long long q = (n == 1) ? 0 : e * (4 / n);
+    *c = cs[q][0];
+    *s = cs[q][1];
+    return;
+  }
+  const long long n8 = n >> 3;
+  const long long oct = e / n8;
+  const long long r = e - oct * n8;
+  // angle theta = 2 pi e / n = (pi/4) * oct + phi, phi = 2 pi r / n in [0, pi/4)
+  auto base = [&](long long rr, double* cc, double* ss) {
+    const double phi = 2.0 * M_PI * (double)rr / (double)n;
+    *cc = std::cos(phi);
+    *ss = std::sin(phi);
+  };
+  double cr, sr, cq, sq;
+  base(r, &cr, &sr);          // cos/sin(phi)
+  base(n8 - r, &cq, &sq);     // cos/sin(pi/4 - phi)
+  double C, S;                // cos/sin(theta)
+  switch (oct) {
+    case 0: C = cr; S = sr; break;
+    case 1: C = sq; S = cq; break;        // theta = pi/2 - (pi/4 - phi)
+    case 2: C = -sr; S = cr; break;       // theta = pi/2 + phi
+    case 3: C = -cq; S = sq; break;       // theta = pi - (pi/4 - phi)
+    case 4: C = -cr; S = -sr; break;      // theta = pi + phi
+    case 5: C = -sq; S = -cq; break;
+    case 6: C = sr; S = -cr; break;       // theta = 3pi/2 + phi
+    default: C = cq; S = -sq; break;      // theta = 2pi - (pi/4 - phi)
+  }
+  if (r == 0) {  // exact octant points
+    const double h = std::sqrt(0.5);
+    static const double ex[8][2] = {{1, 0}, {0, 0}, {0, 1}, {0, 0}, {-1, 0}, {0, 0}, {0, -1}, {0, 0}};
+    if ((oct & 1) == 0) { C = ex[oct][0]; S = ex[oct][1]; }
+    else {
+      C = (oct == 1 || oct == 7) ? h : -h;
+      S = (oct == 1 || oct == 3) ? h : -h;
+    }
+  }
+  *c = C;
+  *s = (S == 0.0) ? 0.0 : -S;  // exp(-i theta), without negative zeros
+}
+
+const float2* twiddle_pyramid(int max_log, cudaStream_t stream) {
+  int dev = 0;
+  cudaGetDevice(&dev);
+  std::lock_guard<std::mutex> lk(g_tw_mu);
+  if ((int)g_tw.size() <= dev) g_tw.resize(dev + 1);
+  Pyramid& p = g_tw[dev];
+  const int want = max_log < 18 ? 18 : max_log;
+  if (p.dev && p.max_log >= want) return p.dev;
+  const size_t total = ((size_t)1 << (want + 1)) - 1;
+  std::vector<float2> host(total);
+  for (int L = 0; L <= want; ++L) {
+    const size_t off = ((size_t)1 << L) - 1;
+    for (long long e = 0; e < (1LL << L); ++e) {
+      double c, s;
+      octant_value(e, L, &c, &s);
+      host[off + e] = make_float2((float)c, (float)s);
+    }
+  }
+  float2* d = nullptr;
+  if (cudaMalloc(&d, total * sizeof(float2)) != cudaSuccess) return p.dev;
+  cudaMemcpyAsync(d, host.data(), total * sizeof(float2), cudaMemcpyHostToDevice, stream);
+  cudaStreamSynchronize(stream);
+  // The previous (smaller) table stays allocated: kernels still queued on
+  // other streams may read it.
+  p.dev = d;
+  p.max_log = want;
+  return p.dev;
+}
+
+
+namespace {
+std::vector<float2*> g_pass;  // per device, guarded by g_tw_mu
+}
+
+// Per-pass twiddle tables (layout in fft_engine.cuh, pass_table_offset):
+// w[(r-1)*Ns + k] = exp(-2 pi i k r / (Ns R)), built in FP64 with the same
+// octant symmetry as the pyramid.
+const float2* twiddle_pass_tables(cudaStream_t stream) {
+  int dev = 0;
+  cudaGetDevice(&dev);
+  std::lock_guard<std::mutex> lk(g_tw_mu);
+  if ((int)g_pass.size() <= dev) g_pass.resize(dev + 1, nullptr);
+  if (g_pass[dev]) return g_pass[dev];
+  const long long total = pass_table_size();
+  std::vector<float2> host((size_t)total);
+  for (int lr = 1; lr <= 4; ++lr) {
+    const int R = 1 << lr;
+    for (int lns = 0; lns <= kPassMaxLog; ++lns) {
+      const long long Ns = 1LL << lns;
+      const long long off = pass_table_offset(lr, lns);
+      for (int r = 1; r < R; ++r)
+        for (long long k = 0; k < Ns; ++k) {
+          double c, s;
+          octant_value(k * r, lns + lr, &c, &s);
+          host[(size_t)(off + (r - 1) * Ns + k)] = make_float2((float)c, (float)s);
+        }
+    }
+  }
+  float2* d = nullptr;
+  if (cudaMalloc(&d, host.size() * sizeof(float2)) != cudaSuccess) return nullptr;
+  cudaMemcpyAsync(d, host.data(), host.size() * sizeof(float2), cudaMemcpyHostToDevice, stream);
+  cudaStreamSynchronize(stream);
+  g_pass[dev] = d;
+  return d;
+}
+
+}  // namespace ffb

@@ -90,4 +90,16 @@ cudaError_t launch_c2c(const C2cArgs& a, int logr, cudaStream_t s, uint64_t* lau
 cudaError_t launch_cplx_batch(const CplxBatchArgs& a, int logr, cudaStream_t s, uint64_t* launches);
 cudaError_t launch_ola(const OlaArgs& a, cudaStream_t s, uint64_t* launches);
 
+// Multi-pass (four-step) transforms for 2^14 <= N <= 2^20.  `scratch` holds
+// `chunk` transforms of N complex points (four_step_chunk picks a chunk
+// that stays resident in L2).
+int max_multi_pass_log();
+size_t four_step_chunk(int log_n, long long batch);
+cudaError_t launch_four_step_stft(const StftArgs& a, float2* scratch, size_t chunk, cudaStream_t s,
+                                  uint64_t* launches);
+cudaError_t launch_four_step_c2c(const C2cArgs& a, float2* scratch, size_t chunk, cudaStream_t s,
+                                 uint64_t* launches);
+cudaError_t launch_four_step_cplx(const CplxBatchArgs& a, float2* scratch, size_t chunk, cudaStream_t s,
+                                  uint64_t* launches);
+
 }  // namespace ffb

@@ -245,3 +245,67 @@ def test_deterministic_repeat():
     b, _ = run_batched(kw, pcm)
     for x, y in zip(a, b):
         assert np.array_equal(x, y)
+
+
+# -- multi-pass (four-step) sizes ---------------------------------------------
+@pytest.mark.parametrize("N", [1 << 14, 1 << 15, 1 << 16, 1 << 17, 1 << 18, 1 << 20])
+@pytest.mark.parametrize("kernel,inverse,transform,half,polar", [(2, 0, 0, 0, 0), (0, 1, 0, 0, 0),
+                                                                  (0, 0, 1, 1, 1), (2, 1, 2, 1, 0)])
+def test_c2c_multipass(N, kernel, inverse, transform, half, polar):
+    B = max(1, (1 << 17) // N)
+    rng = np.random.default_rng(N + 7 * transform)
+    x = (rng.standard_normal((B, N)) + 1j * rng.standard_normal((B, N))).astype(np.complex64)
+    ctx = ff.FftContext.full_v2(N, kernel=kernel, inverse=inverse, transform=transform, half_spectrum=half,
+                                store_polar=polar)
+    out = np.zeros_like(x)
+    assert ctx.execute_c2c(x.view(np.float32), out.view(np.float32), B) == 1
+    _, ref, _ = OracleContext(N=N, kernel=kernel, inverse=inverse, transform=transform, half_spectrum=half,
+                              store_polar=polar).fft_columns(x)
+    if polar:
+        assert_close(out.real * np.exp(1j * out.imag.astype(np.float64)),
+                     ref.real * np.exp(1j * ref.imag.astype(np.float64)), tol_for(N), "polar value")
+    else:
+        assert_close(out, ref, tol_for(N))
+
+
+def test_c2c_multipass_chunks():
+    # N = 65536: the L2-sized scratch holds 64 transforms, so 130 spans 3 chunks
+    N, B = 1 << 16, 130
+    rng = np.random.default_rng(5)
+    x = (rng.standard_normal((B, N)) + 1j * rng.standard_normal((B, N))).astype(np.complex64)
+    ctx = ff.FftContext.full_v2(N, kernel=2)
+    out = np.zeros_like(x)
+    assert ctx.execute_c2c(x.view(np.float32), out.view(np.float32), B) == 1
+    rows = [0, 63, 64, 100, 129]
+    _, ref, _ = OracleContext(N=N, kernel=2).fft_columns(x[rows])
+    assert_close(out[rows], ref, tol_for(N))
+
+
+@pytest.mark.parametrize("N", [1 << 15, 1 << 16, 1 << 17])
+@pytest.mark.parametrize("opts", [dict(transform=1, half_spectrum=1, reduce_magnitude=1),
+                                  dict(transform=1, half_spectrum=1, store_polar=1, apply_windows=1,
+                                       analysis_kind=1),
+                                  dict(transform=0, half_spectrum=0, kernel=2, inverse=1)])
+def test_stft_multipass(N, opts):
+    kw = ctx_kwargs(N, window=N, hop=N // 4, **opts)
+    pcm = np.random.default_rng(N).uniform(-1, 1, 2 * N + 100).astype(np.float32)
+    got, ref = run_batched(kw, pcm)
+    compare_spectrum(kw, got, ref, tol_for(N))
+
+
+@pytest.mark.parametrize("N", [1 << 14, 1 << 15, 1 << 16])
+@pytest.mark.parametrize("ola", [0, 1])
+def test_complex_batched_multipass(N, ola):
+    kw = ctx_kwargs(N, transform=2, half_spectrum=1, store_polar=1, inverse=1, window=N, hop=N // 2,
+                    apply_windows=1, apply_ola=ola, analysis_kind=1, synthesis_kind=1, cola_mode=1)
+    ctx = ff.FftContext.full_v2(**kw)
+    ref = oracle_for(kw)
+    frames = 3
+    bins = N // 2 + 1
+    rng = np.random.default_rng(N + ola)
+    re = np.abs(rng.standard_normal(frames * bins)).astype(np.float32)
+    im = rng.uniform(-np.pi, np.pi, frames * bins).astype(np.float32)
+    out = np.zeros(frames * N, np.float32)
+    assert ctx.execute_complex_batched(re, im, frames, out) == frames
+    _, rout = ref.execute_complex_batched(re, im, frames)
+    assert_close(out, rout.ravel(), tol_for(N))
