@@ -22,6 +22,7 @@ data-path collective); time is the max over ranks.
 from __future__ import annotations
 
 import argparse
+import math
 import json
 import os
 import statistics
@@ -359,7 +360,55 @@ def measure_legs(ff, torch, stream, reps: int = 10):
     legs["stft_r2c_n1024_h256_long_signal"]["frames_per_s"] = round(
         frames / (legs["stft_r2c_n1024_h256_long_signal"]["ms"] * 1e-3), 1)
     c.close()
+    legs["autograd_stft_magnitude"] = measure_autograd(torch, stream, timed)
     return legs
+
+
+def measure_autograd(torch, stream, timed):
+    """Differentiation workload: 64 signals x 262,144 samples (8 sinusoids,
+    frequency U(0, fs/2), amplitude U[0.1, 1], phase U[0, 2 pi), plus N(0, 0.01)
+    noise, seed 4), Hann W = N = 2048, H = 512 (509 frames x 1025 bins).
+    Plain forward = the magnitude STFT kernel alone; fwd+bwd = the
+    torch.autograd.Function forward and backward for a given upstream
+    gradient; with_loss adds sum((|X| - T)^2) and its torch elementwise ops."""
+    from fftfree_b200 import autograd as ag
+
+    S, L, N, H = 64, 262144, 2048, 512
+    g = torch.Generator(device="cuda").manual_seed(4)
+    t = torch.arange(L, device="cuda", dtype=torch.float32)
+    x = torch.zeros(S, L, device="cuda")
+    for _ in range(8):
+        f = torch.rand(S, 1, device="cuda", generator=g) * 0.5
+        a = torch.rand(S, 1, device="cuda", generator=g) * 0.9 + 0.1
+        ph = torch.rand(S, 1, device="cuda", generator=g) * (2 * math.pi)
+        x += a * torch.sin(2 * math.pi * f * t + ph)
+    x += 0.1 * torch.randn(S, L, device="cuda", generator=g)
+    plan = ag.StftPlan(N, H, N, "hann")
+    F = plan.frames(L)
+    bins = plan.bins
+    target = plan.magnitude(x.roll(1, 0)).detach()
+    upstream = torch.randn(S, F, bins, device="cuda", generator=g)
+    in_b, mag_b = S * L * 4, S * F * bins * 4
+    fwd = timed(lambda: plan.magnitude(x), in_b + mag_b)
+    bwd = timed(lambda: plan.magnitude_backward(x, upstream), 2 * in_b + mag_b)
+    xr = x.detach().clone().requires_grad_(True)
+
+    def fwd_bwd():
+        xr.grad = None
+        ag.stft_magnitude(xr, plan).backward(upstream)
+
+    def with_loss():
+        xr.grad = None
+        (ag.stft_magnitude(xr, plan) - target).square().sum().backward()
+
+    fb = timed(fwd_bwd, 3 * in_b + 2 * mag_b)
+    fl = timed(with_loss, 3 * in_b + 2 * mag_b)
+    plan.close()
+    return {"signals": S, "samples": L, "n_fft": N, "hop": H, "frames": F, "bins": bins,
+            "fwd": fwd, "bwd": bwd, "fwd_bwd": fb, "fwd_bwd_with_loss": fl,
+            "ratio_fwd_bwd_over_fwd": round(fb["ms"] / fwd["ms"], 3),
+            "ratio_with_loss_over_fwd": round(fl["ms"] / fwd["ms"], 3),
+            "frames_per_s_fwd": round(S * F / (fwd["ms"] * 1e-3), 1)}
 
 
 if __name__ == "__main__":

@@ -99,6 +99,10 @@ _SIGS = [
     ("fftfree_device_available", ctypes.c_int, []),
     ("fftfree_execute_complex_batched_noalloc", ctypes.c_size_t, [ctypes.c_void_p, c_float_p, c_float_p,
                                                                    ctypes.c_size_t, c_float_p, ctypes.c_size_t]),
+    ("fftfree_stft_magnitude", ctypes.c_size_t, [ctypes.c_void_p, c_float_p, ctypes.c_size_t, ctypes.c_size_t,
+                                                 c_float_p, ctypes.c_size_t]),
+    ("fftfree_stft_magnitude_backward", ctypes.c_size_t, [ctypes.c_void_p, c_float_p, ctypes.c_size_t,
+                                                          ctypes.c_size_t, c_float_p, c_float_p]),
     ("fftfree_debug_recovery_plan", ctypes.c_size_t, [ctypes.c_size_t, ctypes.c_char_p]),
 ]
 
@@ -249,6 +253,14 @@ class FftContext:
             else:  # torch tensor: complex dtype, or interleaved floats
                 arr[i].count = buf.numel() if buf.is_complex() else buf.numel() // 2
         return int(lib().fftfree_execute_c2c_meta(self.handle, _fp(x), _fp(out), batch, arr, len(requests)))
+
+
+    def stft_magnitude(self, pcm, signals, length, out_mag, max_frames=0) -> int:
+        return int(lib().fftfree_stft_magnitude(self.handle, _fp(pcm), signals, length, _fp(out_mag), max_frames))
+
+    def stft_magnitude_backward(self, pcm, signals, length, grad_mag, grad_pcm) -> int:
+        return int(lib().fftfree_stft_magnitude_backward(self.handle, _fp(pcm), signals, length, _fp(grad_mag),
+                                                         _fp(grad_pcm)))
 
 
 def device_available() -> bool:

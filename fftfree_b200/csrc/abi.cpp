@@ -266,8 +266,10 @@ static bool single_pass(int N, bool real_input) {
 
 static float2* scratch_for(FftContext* c, int N, long long batch, size_t* chunk) {
   *chunk = four_step_chunk(ilog2((size_t)N), batch);
-  // two slots: the multi-pass pipeline alternates between them
-  return static_cast<float2*>(c->d_scratch.get(2 * *chunk * (size_t)N * sizeof(float2)));
+  // two slots when the multi-pass pipeline alternates between chunks,
+  // one when a single chunk covers the batch
+  const size_t slots = ((long long)*chunk < batch) ? 2 : 1;
+  return static_cast<float2*>(c->d_scratch.get(slots * *chunk * (size_t)N * sizeof(float2)));
 }
 
 static void setup_device(FftContext* c) {
@@ -930,6 +932,111 @@ FFT_CFFI_API int fftfree_execute_c2c_meta(void* handle, const float* in, float* 
     std::lock_guard<std::recursive_mutex> lk(c->mu);
     DeviceGuard g(c->device);
     return run_meta(c, in, out, batch, requests, request_count);
+  } catch (...) {
+    return 0;
+  }
+}
+
+// ------------------------------------------------------------------ gradients
+// Magnitude STFT of `signals` signals (row stride `length`) and its
+// gradient; the context fixes N, window, hop, pad rule and analysis window.
+static bool mag_grad_ctx_ok(const FftContext* c, const char* who) {
+  const bool ok = !c->inverse && c->eff_transform() == FFT_TRANSFORM_R2C && c->half_spectrum &&
+                  c->N >= 2 && ilog2((size_t)c->N) <= max_mag_grad_log();
+  if (!ok)
+    std::fprintf(stderr, "[fftfree_b200] %s: needs a forward R2C half-spectrum context with 2 <= N <= %d\n",
+                 who, 1 << max_mag_grad_log());
+  return ok;
+}
+
+static int mag_grad_span(int H) {
+  static const int env = [] {
+    const char* e = std::getenv("FFTFREE_GRAD_SPAN");
+    return e ? std::atoi(e) : 0;
+  }();
+  if (env > 0) return env;
+  // about 16 hops of one signal per block, at least one hop
+  long long s = 16LL * H;
+  if (s > 8192) s = std::max(8192, H);
+  return (int)s;
+}
+
+FFT_CFFI_API size_t fftfree_stft_magnitude(void* handle, const float* pcm, size_t signals, size_t length,
+                                           float* out_mag, size_t max_frames) {
+  FftContext* c = as_ctx(handle);
+  if (!c || !pcm || !out_mag || signals == 0 || length == 0) return 0;
+  try {
+    std::lock_guard<std::recursive_mutex> lk(c->mu);
+    if (!mag_grad_ctx_ok(c, "fftfree_stft_magnitude")) return 0;
+    DeviceGuard g(c->device);
+    const size_t frames = frame_count(c, length, 0, max_frames);
+    if (frames == 0) return 0;
+    const int W = c->window ? c->window : c->N;
+    const int H = c->hop ? c->hop : W;
+    const int bins = c->N / 2 + 1;
+    bool any_host = !is_device_ptr(pcm);
+    const float* d_pcm = stage_in(c, c->d_in0, pcm, signals * length);
+    OutTarget o = stage_out(c->d_out2, out_mag, signals * frames * (size_t)bins);
+    any_host = any_host || o.host;
+    StftArgs a{};
+    a.pcm = d_pcm;
+    a.pcm_len = (long long)length;
+    a.frames = (long long)(signals * frames);
+    a.N = c->N;
+    a.W = W;
+    a.H = H;
+    a.win = c->windows_enabled ? static_cast<const float*>(c->d_analysis.p) : nullptr;
+    a.pf = c->post_flags();
+    a.out_bins = bins;
+    a.out_stride = bins;
+    a.out_mag = o.dev;
+    a.sig_frames = (long long)frames;
+    a.sig_stride = (long long)length;
+    a.mag_only = 1;
+    FFB_CHECK(launch_stft(a, c->logr_req, c->stream, &c->launches));
+    finish_out(c, o);
+    finish_call(c, any_host);
+    return frames;
+  } catch (...) {
+    return 0;
+  }
+}
+
+FFT_CFFI_API size_t fftfree_stft_magnitude_backward(void* handle, const float* pcm, size_t signals,
+                                                    size_t length, const float* grad_mag, float* grad_pcm) {
+  FftContext* c = as_ctx(handle);
+  if (!c || !pcm || !grad_mag || !grad_pcm || signals == 0 || length == 0) return 0;
+  try {
+    std::lock_guard<std::recursive_mutex> lk(c->mu);
+    if (!mag_grad_ctx_ok(c, "fftfree_stft_magnitude_backward")) return 0;
+    DeviceGuard g(c->device);
+    const size_t frames = frame_count(c, length, 0, 0);
+    if (frames == 0) return 0;
+    const int W = c->window ? c->window : c->N;
+    const int H = c->hop ? c->hop : W;
+    const int bins = c->N / 2 + 1;
+    bool any_host = !is_device_ptr(pcm) || !is_device_ptr(grad_mag);
+    const float* d_pcm = stage_in(c, c->d_in0, pcm, signals * length);
+    const float* d_g = stage_in(c, c->d_in1, grad_mag, signals * frames * (size_t)bins);
+    OutTarget o = stage_out(c->d_out0, grad_pcm, signals * length);
+    any_host = any_host || o.host;
+    MagGradArgs a{};
+    a.pcm = d_pcm;
+    a.signals = (long long)signals;
+    a.pcm_len = (long long)length;
+    a.sig_stride = (long long)length;
+    a.frames = (long long)frames;
+    a.N = c->N;
+    a.W = W;
+    a.H = H;
+    a.win = c->windows_enabled ? static_cast<const float*>(c->d_analysis.p) : nullptr;
+    a.grad_mag = d_g;
+    a.grad_pcm = o.dev;
+    a.span = mag_grad_span(H);
+    FFB_CHECK(launch_stft_mag_grad(a, c->logr_req, c->stream, &c->launches));
+    finish_out(c, o);
+    finish_call(c, any_host);
+    return frames;
   } catch (...) {
     return 0;
   }

@@ -70,7 +70,27 @@ __device__ __forceinline__ float2 post_hook_m(float2 X, int k, int N, const Post
 
 __host__ __device__ inline int post_mode(const PostFlags& pf) { return pf.polar ? 2 : (pf.reduce ? 1 : 0); }
 
+// Frame f of a (possibly multi-signal) STFT: its first sample and how many
+// samples it takes from the signal (fft_cffi.cpp:765-791: frame f covers
+// pcm[f*H .. f*H + W), zero beyond the signal end and from W up to N).
+__device__ __forceinline__ const float* stft_frame(const float* pcm, long long pcm_len, long long sig_frames,
+                                                   long long sig_stride, int W, int H, long long f,
+                                                   long long* cnt) {
+  if (sig_frames > 0) {
+    const long long s = f / sig_frames;
+    pcm += s * sig_stride;
+    f -= s * sig_frames;
+  }
+  const long long start = f * (long long)H;
+  long long c = pcm_len - start;
+  if (c > W) c = W;
+  *cnt = c;
+  return pcm + start;
+}
+
 // ------------------------------------------------------------------ STFT IO
+// MODE: 0 plain / imag clear, 1 reduce_magnitude, 2 store_polar, 3 |X| only
+// (forward half spectrum, magnitude array alone).
 template <int MODE>
 struct StftIO {
   StftArgs a;
@@ -83,13 +103,10 @@ struct StftIO {
       for (int i = 0; i < S::R; ++i) v[i] = make_float2(0.f, 0.f);
       return;
     }
-    // fft_cffi.cpp:765-791 framing: frame f covers pcm[f*H .. f*H + W), zero
-    // beyond the signal end and from W up to N; Cooley-Tukey C2R half adds the
-    // pre-hook's mirror (eigen_fft.hpp:2523-2528), x[N-n] = x[n] on real frames.
-    const long long start = f * (long long)a.H;
-    long long cnt = a.pcm_len - start;
-    if (cnt > a.W) cnt = a.W;
-    const float* src = a.pcm + start;
+    // Cooley-Tukey C2R half adds the pre-hook's mirror (eigen_fft.hpp:2523-2528),
+    // x[N-n] = x[n] on real frames.
+    long long cnt;
+    const float* src = stft_frame(a.pcm, a.pcm_len, a.sig_frames, a.sig_stride, a.W, a.H, f, &cnt);
     if (a.N == 1) {
       const float s = (cnt > 0) ? __ldg(src) : 0.f;
 #pragma unroll
@@ -135,11 +152,10 @@ struct StftIO {
     if (f >= a.frames) return make_float2(0.f, 0.f);
     int nn = (int)n;
     if (a.mirror && nn > (a.N >> 1)) nn = a.N - nn;
-    const long long start = f * (long long)a.H;
-    long long cnt = a.pcm_len - start;
-    if (cnt > a.W) cnt = a.W;
+    long long cnt;
+    const float* src = stft_frame(a.pcm, a.pcm_len, a.sig_frames, a.sig_stride, a.W, a.H, f, &cnt);
     if ((long long)nn >= cnt) return make_float2(0.f, 0.f);
-    float s = __ldg(a.pcm + start + nn);
+    float s = __ldg(src + nn);
     if (a.win) s *= __ldg(a.win + nn);
     return make_float2(s, 0.f);
   }
@@ -147,8 +163,8 @@ struct StftIO {
     if (f >= a.frames || k >= a.out_bins) return;
     const long long ob = f * a.out_stride;
     const bool mag_is_re = (MODE == 1) || (MODE == 2 && a.mag_from_real);
-    emit(a.out_re + ob, a.out_im + ob, a.out_mag + ob, (int)k, X, k == 0 || 2 * k == a.N,
-         1.0f / (float)a.N, mag_is_re);
+    emit(a.out_re + (MODE == 3 ? 0 : ob), a.out_im + (MODE == 3 ? 0 : ob), a.out_mag + ob, (int)k, X,
+         k == 0 || 2 * k == a.N, 1.0f / (float)a.N, mag_is_re);
   }
 
   // Bin k of the output: inverse scaling, exact-real DC / Nyquist, post
@@ -159,6 +175,10 @@ struct StftIO {
     // Real input: DC and Nyquist are exactly real (imag +0), as in the
     // reference's radix-2 executors.
     if (dc_or_nyq) X.y = 0.f;
+    if constexpr (MODE == 3) {
+      mg[k] = cabs_fast(X.x, X.y);
+      return;
+    }
     X = post_hook_m<MODE>(X, k, a.N, a.pf);
     re[k] = X.x;
     im[k] = X.y;
@@ -173,8 +193,8 @@ struct StftIO {
     __syncthreads();
     if (f >= a.frames) return;
     const long long ob = f * a.out_stride;
-    float* re = a.out_re + ob;
-    float* im = a.out_im + ob;
+    float* re = a.out_re + (MODE == 3 ? 0 : ob);
+    float* im = a.out_im + (MODE == 3 ? 0 : ob);
     float* mg = a.out_mag + ob;
     const bool mag_is_re = (MODE == 1) || (MODE == 2 && a.mag_from_real);
     if (a.N == 1) {
@@ -200,6 +220,10 @@ struct StftIO {
         const float2 O = make_float2(0.5f * D.y, -0.5f * D.x);
         float2 X = cadd(E, cmul(__ldg(w + i * T), O));
         if (i == 0 && t == 0) X.y = 0.f;  // DC
+        if constexpr (MODE == 3) {
+          pm[i * T] = cabs_fast(X.x, X.y);
+          continue;
+        }
         float mag;
         if constexpr (MODE == 2) { mag = cabs_fast(X.x, X.y); X = make_float2(mag, atan2f(X.y, X.x)); }
         else if constexpr (MODE == 1) { mag = cabs_fast(X.x, X.y); X = make_float2(mag, 0.f); }

@@ -1,0 +1,268 @@
+// k_grad.cu -- gradient of the magnitude STFT with respect to the signals
+// (the adjoint of the forward R2C half-spectrum STFT followed by |.|).
+//
+// For one frame s[n] = x[f*H + n] * w[n] (zero from the frame's sample
+// count on) with half spectrum X[k], k = 0..N/2, and upstream gradient
+// g[k] = dL/d|X[k]|:
+//   dL/ds[n] = Re sum_{k=0}^{N/2} V[k] e^{+2 pi i k n / N},  V[k] = g[k] X[k] / |X[k]|
+// (V = 0 where |X| = 0), i.e. the unnormalised Hermitian inverse of the
+// half spectrum Y with Y[k] = V[k] for 0 < k < N/2 and Y[0] = 2 Re V[0],
+// Y[N/2] = 2 Re V[N/2], halved -- computed as one N/2-point complex
+// transform.  dL/dx[t] = sum over the frames f covering t of
+// w[t - f*H] * dL/ds_f[t - f*H].
+//
+// The spectrum is recomputed from x rather than stored by the forward
+// pass.  Each block owns `span` consecutive samples of one signal and
+// transforms every frame that touches them (a few frames of halo per block
+// are transformed by both neighbours); the overlap-add adjoint is a gather
+// in frame order through a shared-memory accumulator, so the result is
+// deterministic and needs no atomics.
+#include "fft_launch.cuh"
+
+namespace ffb {
+namespace {
+
+template <class S>
+struct SchedTag {
+  using type = S;
+};
+
+template <int LOGM, class F>
+cudaError_t with_r(int logr, F&& f) {
+  switch (logr) {
+    case 2: return f(SchedTag<Sched<LOGM, 2>>{});
+    case 3: return f(SchedTag<Sched<LOGM, 3>>{});
+    default: return f(SchedTag<Sched<LOGM, 4>>{});
+  }
+}
+
+template <class F>
+cudaError_t with_sched(int logm, int logr, F&& f) {
+  switch (logm) {
+    case 0: return with_r<0>(logr, f);
+    case 1: return with_r<1>(logr, f);
+    case 2: return with_r<2>(logr, f);
+    case 3: return with_r<3>(logr, f);
+    case 4: return with_r<4>(logr, f);
+    case 5: return with_r<5>(logr, f);
+    case 6: return with_r<6>(logr, f);
+    case 7: return with_r<7>(logr, f);
+    case 8: return with_r<8>(logr, f);
+    case 9: return with_r<9>(logr, f);
+    case 10: return with_r<10>(logr, f);
+    case 11: return with_r<11>(logr, f);
+    case 12: return with_r<12>(logr, f);
+    case 13: return with_r<13>(logr, f);
+    default: return cudaErrorInvalidValue;
+  }
+}
+
+// Frame f of one signal as M complex points z[m] = (s[2m], s[2m+1]).
+template <class S>
+__device__ __forceinline__ void grad_load(const MagGradArgs& a, const float* pcm, long long f, bool ok, int t,
+                                          float2 (&v)[S::R], long long* cnt_out) {
+  long long cnt = 0;
+  const float* src = ok ? stft_frame(pcm, a.pcm_len, 0, 0, a.W, a.H, f, &cnt) : pcm;
+  *cnt_out = cnt;
+  if (!ok) {
+#pragma unroll
+    for (int i = 0; i < S::R; ++i) v[i] = make_float2(0.f, 0.f);
+    return;
+  }
+  if (cnt == a.N && aligned8(src) && (!a.win || aligned8(a.win))) {
+    const float2* s2 = reinterpret_cast<const float2*>(src);
+    const float2* w2 = reinterpret_cast<const float2*>(a.win);
+#pragma unroll
+    for (int i = 0; i < S::R; ++i) {
+      const int m = t + i * S::T;
+      float2 z = __ldg(s2 + m);
+      if (w2) z = __fmul2_rn(z, __ldg(w2 + m));
+      v[i] = z;
+    }
+    return;
+  }
+#pragma unroll
+  for (int i = 0; i < S::R; ++i) {
+    const int n = 2 * (t + i * S::T);
+    float x0 = 0.f, x1 = 0.f;
+    if (n < cnt) x0 = a.win ? __ldg(src + n) * __ldg(a.win + n) : __ldg(src + n);
+    if (n + 1 < cnt) x1 = a.win ? __ldg(src + n + 1) * __ldg(a.win + n + 1) : __ldg(src + n + 1);
+    v[i] = make_float2(x0, x1);
+  }
+}
+
+// dL/dX scaled onto the Hermitian half spectrum: V = g X / |X|, 0 at |X| = 0.
+__device__ __forceinline__ float2 mag_chain(float2 X, float g) {
+  const float m = cabs_fast(X.x, X.y);
+  if (!(m > 0.f)) return make_float2(0.f, 0.f);
+  const float s = g / m;
+  return make_float2(X.x * s, X.y * s);
+}
+
+template <class S>
+__global__ void __launch_bounds__(Launch<S>::BLOCK) k_stft_mag_grad(MagGradArgs a, Twiddles tw) {
+  extern __shared__ float2 smem[];
+  constexpr int T = S::T, R = S::R, M = S::M;
+  constexpr int G = Launch<S>::G, B = Launch<S>::BLOCK;
+  constexpr int LN = S::LOGM + 1;  // N = 2M
+  const int g = threadIdx.x / T;
+  const int t = threadIdx.x - g * T;
+  float2* sm = smem + g * S::SMEM;
+  float* acc = reinterpret_cast<float*>(smem + G * S::SMEM);
+
+  const long long per_sig = (a.pcm_len + a.span - 1) / a.span;
+  const long long sig = blockIdx.x / per_sig;
+  const long long s0 = (blockIdx.x - sig * per_sig) * (long long)a.span;
+  const long long s1 = (s0 + a.span < a.pcm_len) ? s0 + a.span : a.pcm_len;
+  const int ns = (int)(s1 - s0);
+  for (int p = threadIdx.x; p < ns; p += B) acc[p] = 0.f;
+
+  // frames f with f*H < s1 and f*H + W > s0 (fewer samples only at the end)
+  const long long f_lo = (s0 >= a.W) ? (s0 - a.W) / a.H + 1 : 0;
+  long long f_hi = (s1 - 1) / a.H;
+  if (f_hi > a.frames - 1) f_hi = a.frames - 1;
+  const float* pcm = a.pcm + sig * a.sig_stride;
+  const float* gsig = a.grad_mag + sig * a.frames * (long long)(M + 1);
+  const float2* w = tw.pyr + ((1 << LN) - 1) + t;  // e^{-2 pi i k / N}, k = t + i*T
+  __syncthreads();
+
+  for (long long f0 = f_lo; f0 <= f_hi; f0 += G) {  // block-uniform loop
+    const long long f = f0 + g;
+    const bool ok = f <= f_hi;
+    float2 v[R];
+    long long cnt;
+    grad_load<S>(a, pcm, f, ok, t, v, &cnt);
+    fft_engine<S>(v, t, sm, tw);
+
+    // Untangle Z (the M-point transform of z) into X[k], k = t + i*T, and
+    // apply the magnitude chain rule bin by bin.
+    tile_write_natural<S>(v, t, sm);
+    __syncthreads();
+    const float* gf = gsig + (ok ? f : 0) * (long long)(M + 1);
+    float2 y[R];
+#pragma unroll
+    for (int i = 0; i < R; ++i) {
+      const int k = t + i * T;
+      const float2 zk = v[i];
+      const float2 zm = sm[pidx((M - k) & (M - 1))];
+      const float2 E = make_float2(0.5f * (zk.x + zm.x), 0.5f * (zk.y - zm.y));
+      const float2 D = make_float2(zk.x - zm.x, zk.y + zm.y);
+      const float2 O = make_float2(0.5f * D.y, -0.5f * D.x);
+      float2 X = cadd(E, cmul(__ldg(w + i * T), O));
+      const float gk = ok ? __ldg(gf + k) : 0.f;
+      if (i == 0 && t == 0) {
+        X.y = 0.f;  // DC is real
+        const float2 V = mag_chain(X, gk);
+        y[i] = make_float2(2.f * V.x, 0.f);
+      } else {
+        y[i] = mag_chain(X, gk);
+      }
+    }
+    float2 ynyq = make_float2(0.f, 0.f);
+    if (t == 0) {  // Nyquist X[M] = Re Z[0] - Im Z[0]
+      const float xn = v[0].x - v[0].y;
+      const float gn = ok ? __ldg(gf + M) : 0.f;
+      ynyq = make_float2(2.f * mag_chain(make_float2(xn, 0.f), gn).x, 0.f);
+    }
+    __syncthreads();  // every read of Z is done
+    tile_write_natural<S>(y, t, sm);
+    if (t == 0) sm[pidx(M)] = ynyq;
+    __syncthreads();
+
+    // Hermitian half spectrum Y -> z' with x[2m] = Re, x[2m+1] = Im of the
+    // unnormalised inverse: E = (Y[m] + conj Y[M-m]) / 2,
+    // O = (Y[m] - conj Y[M-m]) e^{+2 pi i m/N} / 2, z' = IDFT_M(E + i O),
+    // the IDFT taken as conj . DFT . conj.
+#pragma unroll
+    for (int i = 0; i < R; ++i) {
+      const int m = t + i * T;
+      const float2 ym = sm[pidx(M - m)];
+      const float2 E = make_float2(0.5f * (y[i].x + ym.x), 0.5f * (y[i].y - ym.y));
+      const float2 D = make_float2(0.5f * (y[i].x - ym.x), 0.5f * (y[i].y + ym.y));
+      const float2 O = cmul(D, cconj(__ldg(w + i * T)));
+      v[i] = make_float2(E.x - O.y, -(E.y + O.x));
+    }
+    __syncthreads();  // the engine reuses the tile
+    fft_engine<S>(v, t, sm, tw);
+
+    // This frame's windowed gradient into its tile: dL/ds[2m] = Re, dL/ds[2m+1] = -Im.
+#pragma unroll
+    for (int i = 0; i < R; ++i) {
+      const int m = t + i * T;
+      const int n = 2 * m;
+      float d0 = v[i].x, d1 = -v[i].y;
+      if (a.win) {
+        d0 *= __ldg(a.win + n);
+        d1 *= __ldg(a.win + n + 1);
+      }
+      if (n >= cnt) d0 = 0.f;
+      if (n + 1 >= cnt) d1 = 0.f;
+      sm[pidx(m)] = make_float2(d0, d1);
+    }
+    __syncthreads();
+
+    // Overlap-add adjoint: each owned sample gathers this round's frames in
+    // frame order.
+    const long long last = (f0 + G - 1 < f_hi) ? f0 + G - 1 : f_hi;
+    long long lo = f0 * (long long)a.H, hi = last * (long long)a.H + a.N;
+    if (lo < s0) lo = s0;
+    if (hi > s1) hi = s1;
+    const int g_last = (int)(last - f0);
+    for (long long p = lo + threadIdx.x; p < hi; p += B) {
+      // frames f0 + gg with 0 <= p - (f0 + gg) * H < N
+      const long long r = p - f0 * (long long)a.H;
+      int gg = (r >= a.N) ? (int)((r - a.N) / a.H) + 1 : 0;
+      int ge = (int)(r / a.H);
+      if (ge > g_last) ge = g_last;
+      float sum = acc[p - s0];
+      for (; gg <= ge; ++gg) {
+        const int n = (int)(r - (long long)gg * a.H);
+        const float* tile = reinterpret_cast<const float*>(smem + gg * S::SMEM);
+        sum += tile[2 * pidx(n >> 1) + (n & 1)];
+      }
+      acc[p - s0] = sum;
+    }
+    __syncthreads();
+  }
+
+  float* out = a.grad_pcm + sig * a.sig_stride + s0;
+  for (int p = threadIdx.x; p < ns; p += B) out[p] = acc[p];
+}
+
+}  // namespace
+
+int max_mag_grad_log() { return 14; }
+
+cudaError_t launch_stft_mag_grad(const MagGradArgs& a, int req_logr, cudaStream_t st, uint64_t* launches) {
+  if (a.N < 2 || (a.N & (a.N - 1)) || a.signals <= 0 || a.pcm_len <= 0 || a.frames <= 0 || a.span <= 0 ||
+      a.H <= 0 || a.W <= 0 || a.W > a.N)
+    return cudaErrorInvalidValue;
+  const int logm = ilog2i(a.N) - 1;
+  if (logm + 1 > max_mag_grad_log()) return cudaErrorInvalidValue;
+  const int logr = choose_logr(logm, req_logr, true);
+  if (logr < 0) return cudaErrorInvalidValue;
+  return with_sched(logm, logr, [&](auto tag) -> cudaError_t {
+    using S = typename decltype(tag)::type;
+    if constexpr (S::T > 1024) {
+      return cudaErrorInvalidValue;
+    } else {
+      using L = Launch<S>;
+      const size_t smem = (size_t)L::G * S::SMEM * sizeof(float2) + (size_t)a.span * sizeof(float);
+      if (smem > 227 * 1024) return cudaErrorInvalidValue;
+      if (smem > 48 * 1024) {
+        const cudaError_t e = cudaFuncSetAttribute(k_stft_mag_grad<S>,
+                                                   cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (e != cudaSuccess) return e;
+      }
+      const long long per_sig = (a.pcm_len + a.span - 1) / a.span;
+      const long long grid = per_sig * a.signals;
+      if (grid > 0x7fffffffLL) return cudaErrorInvalidValue;
+      Twiddles tw{twiddle_pyramid(0, st), twiddle_pass_tables(st)};
+      k_stft_mag_grad<S><<<(unsigned)grid, L::BLOCK, smem, st>>>(a, tw);
+      if (launches) ++*launches;
+      return cudaGetLastError();
+    }
+  });
+}
+
+}  // namespace ffb

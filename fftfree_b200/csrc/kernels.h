@@ -29,9 +29,32 @@ struct StftArgs {
   int out_bins;
   long long out_stride;
   int mag_from_real;  // out_mag = re when store_polar (fft_cffi.cpp:822)
-  float* out_re;
-  float* out_im;
+  float* out_re;   // unused (may be null) with mag_only
+  float* out_im;   // unused (may be null) with mag_only
   float* out_mag;
+  // Several independent signals: frames [s*sig_frames, (s+1)*sig_frames)
+  // read signal s at pcm + s*sig_stride, each `pcm_len` samples long.
+  // sig_frames == 0: one signal.
+  long long sig_frames;
+  long long sig_stride;
+  int mag_only;  // forward R2C half spectrum, only |X| (bins 0..N/2) written
+};
+
+// Gradient of the magnitude STFT (forward R2C half spectrum, |X| per bin)
+// with respect to the signals: recomputes each frame's spectrum, applies
+// the magnitude chain rule, the adjoint transform and the windowed
+// overlap-add adjoint of framing.
+struct MagGradArgs {
+  const float* pcm;       // signals x sig_stride, each pcm_len samples
+  long long signals;
+  long long pcm_len;
+  long long sig_stride;
+  long long frames;       // frames per signal
+  int N, W, H;
+  const float* win;       // device, length >= W, or nullptr
+  const float* grad_mag;  // (signals * frames) x (N/2 + 1)
+  float* grad_pcm;        // signals x sig_stride; every sample < pcm_len written
+  int span;               // samples of one signal owned by one block
 };
 
 // Complex columns in/out with the plan hooks (C++ fft_inplace_batched).
@@ -89,6 +112,9 @@ cudaError_t launch_stft(const StftArgs& a, int logr, cudaStream_t s, uint64_t* l
 cudaError_t launch_c2c(const C2cArgs& a, int logr, cudaStream_t s, uint64_t* launches);
 cudaError_t launch_cplx_batch(const CplxBatchArgs& a, int logr, cudaStream_t s, uint64_t* launches);
 cudaError_t launch_ola(const OlaArgs& a, cudaStream_t s, uint64_t* launches);
+// Largest N (log2) of the magnitude-gradient kernel; 0 for unsupported.
+int max_mag_grad_log();
+cudaError_t launch_stft_mag_grad(const MagGradArgs& a, int logr, cudaStream_t s, uint64_t* launches);
 
 // Multi-pass (four-step) transforms for 2^14 <= N <= 2^20.  `scratch` holds
 // `chunk` transforms of N complex points (four_step_chunk picks a chunk

@@ -87,6 +87,33 @@ FFT_CFFI_API size_t fftfree_execute_complex_batched_noalloc(void* handle, const 
                                                            const float* in_imag, size_t frames,
                                                            float* out_pcm, size_t max_frames);
 
+/* Differentiable STFT magnitude, the forward and adjoint kernels behind a
+ * torch.autograd.Function.  No C counterpart in the reference; it replaces
+ * the forward-STFT approximation of the adjoint that train_mipmap_weights.py
+ * (lines 395-415) uses for its spectral losses.  The context must be a
+ * forward R2C half-spectrum context (fft_init_full / fft_init_full_v2 with
+ * transform=1, half_spectrum=1) with N <= 16384; N, window length W, hop H,
+ * the pad rule of fft_execute_batched (fft_cffi.cpp:710-750) and the
+ * analysis window (apply_windows=1) come from it.
+ *
+ * fftfree_stft_magnitude: |X| of every frame of `signals` signals, each
+ * `length` samples at row stride `length`, into out_mag as
+ * signals x frames x (N/2 + 1) floats (frames per signal as
+ * fft_execute_batched counts them, capped by max_frames when nonzero); the
+ * same framing, window and kernels as fft_execute_batched with
+ * reduce_magnitude.  Returns the frames per signal, 0 on failure. */
+FFT_CFFI_API size_t fftfree_stft_magnitude(void* handle, const float* pcm, size_t signals, size_t length,
+                                           float* out_mag, size_t max_frames);
+
+/* Gradient of sum(grad_mag * |X|) with respect to pcm: grad_mag has the
+ * layout of fftfree_stft_magnitude's output (all frames of every signal),
+ * grad_pcm receives signals x length floats.  The spectrum is recomputed
+ * from pcm, not stored; bins with |X| = 0 contribute nothing; samples no
+ * frame covers get 0.  Deterministic (no atomics).  Returns the frames per
+ * signal, 0 on failure. */
+FFT_CFFI_API size_t fftfree_stft_magnitude_backward(void* handle, const float* pcm, size_t signals,
+                                                    size_t length, const float* grad_mag, float* grad_pcm);
+
 /* Test hook of the recovery coordinator (fft_cffi.cpp:954-982): runs the
  * host-side dropout / restore / split decisions for one batch of `frames`
  * frames, invoking the registered restore observer as the recovery path
