@@ -401,13 +401,24 @@ def measure_autograd(torch, stream, timed):
         xr.grad = None
         (ag.stft_magnitude(xr, plan) - target).square().sum().backward()
 
-    fb = timed(fwd_bwd, 3 * in_b + 2 * mag_b)
-    fl = timed(with_loss, 3 * in_b + 2 * mag_b)
+    # saved phasor (the default at this size): fwd writes |X| and X / |X|, bwd reads g and X / |X|
+    assert plan.stores_phase(xr)
+    fb = timed(fwd_bwd, in_b + 3 * mag_b + 3 * mag_b + in_b)
+    fl = timed(with_loss, in_b + 3 * mag_b + 3 * mag_b + in_b)
+    _, ph = plan.magnitude_phasor(x)
+    bwd_ph = timed(lambda: plan.magnitude_backward_phasor(ph, upstream, L), 3 * mag_b + in_b)
+    plan.close()
+    # recomputed spectrum (the path for signals whose phase exceeds the budget)
+    plan = ag.StftPlan(N, H, N, "hann", phase_budget=0)
+    assert not plan.stores_phase(xr)
+    fb_rc = timed(fwd_bwd, 3 * in_b + 2 * mag_b)
     plan.close()
     return {"signals": S, "samples": L, "n_fft": N, "hop": H, "frames": F, "bins": bins,
-            "fwd": fwd, "bwd": bwd, "fwd_bwd": fb, "fwd_bwd_with_loss": fl,
+            "fwd": fwd, "bwd_recompute": bwd, "bwd_saved_phasor": bwd_ph, "fwd_bwd": fb,
+            "fwd_bwd_with_loss": fl, "fwd_bwd_recompute": fb_rc,
             "ratio_fwd_bwd_over_fwd": round(fb["ms"] / fwd["ms"], 3),
             "ratio_with_loss_over_fwd": round(fl["ms"] / fwd["ms"], 3),
+            "ratio_recompute_over_fwd": round(fb_rc["ms"] / fwd["ms"], 3),
             "frames_per_s_fwd": round(S * F / (fwd["ms"] * 1e-3), 1)}
 
 

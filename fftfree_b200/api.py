@@ -103,6 +103,10 @@ _SIGS = [
                                                  c_float_p, ctypes.c_size_t]),
     ("fftfree_stft_magnitude_backward", ctypes.c_size_t, [ctypes.c_void_p, c_float_p, ctypes.c_size_t,
                                                           ctypes.c_size_t, c_float_p, c_float_p]),
+    ("fftfree_stft_magnitude_phasor", ctypes.c_size_t, [ctypes.c_void_p, c_float_p, ctypes.c_size_t,
+                                                       ctypes.c_size_t, c_float_p, c_float_p, ctypes.c_size_t]),
+    ("fftfree_stft_magnitude_backward_phasor", ctypes.c_size_t, [ctypes.c_void_p, c_float_p, ctypes.c_size_t,
+                                                                ctypes.c_size_t, c_float_p, c_float_p]),
     ("fftfree_debug_recovery_plan", ctypes.c_size_t, [ctypes.c_size_t, ctypes.c_char_p]),
 ]
 
@@ -257,6 +261,14 @@ class FftContext:
 
     def stft_magnitude(self, pcm, signals, length, out_mag, max_frames=0) -> int:
         return int(lib().fftfree_stft_magnitude(self.handle, _fp(pcm), signals, length, _fp(out_mag), max_frames))
+
+    def stft_magnitude_phasor(self, pcm, signals, length, out_mag, out_phasor, max_frames=0) -> int:
+        return int(lib().fftfree_stft_magnitude_phasor(self.handle, _fp(pcm), signals, length, _fp(out_mag),
+                                                       _fp(out_phasor), max_frames))
+
+    def stft_magnitude_backward_phasor(self, phasor, signals, length, grad_mag, grad_pcm) -> int:
+        return int(lib().fftfree_stft_magnitude_backward_phasor(self.handle, _fp(phasor), signals, length,
+                                                                _fp(grad_mag), _fp(grad_pcm)))
 
     def stft_magnitude_backward(self, pcm, signals, length, grad_mag, grad_pcm) -> int:
         return int(lib().fftfree_stft_magnitude_backward(self.handle, _fp(pcm), signals, length, _fp(grad_mag),

@@ -11,6 +11,13 @@
   gather form of the overlap-add adjoint of framing), which recomputes the
   spectrum from the saved signal instead of storing it.
 
+While the saved phasor of a call fits the plan's ``phase_budget`` (bytes),
+the forward pass instead writes the unit phasor X / |X| beside |X|
+(``fftfree_stft_magnitude_phasor``) and the backward starts from it
+(``fftfree_stft_magnitude_backward_phasor``): one transform per frame
+instead of two.  Longer signals keep the recompute path, which stores
+nothing beyond the signal.
+
 Both run on torch's current CUDA stream and never synchronise the host.
 The reference has no autograd path; its ``train_mipmap_weights.py``
 (lines 395-415) approximates the adjoint with a forward STFT.
@@ -36,7 +43,8 @@ class StftPlan:
     (fft_cffi.cpp:163-208, symmetric, denominator W-1) or None for none."""
 
     def __init__(self, n_fft: int, hop: int, win_length: Optional[int] = None, window: Optional[str] = "hann",
-                 window_param: float = 0.0, pad_mode: int = 1, device: Optional[int] = None):
+                 window_param: float = 0.0, pad_mode: int = 1, device: Optional[int] = None,
+                 phase_budget: int = 1 << 30):
         if n_fft < 2 or n_fft & (n_fft - 1) or n_fft > 16384:
             raise ValueError("n_fft must be a power of two in [2, 16384]")
         self.n_fft = int(n_fft)
@@ -45,6 +53,7 @@ class StftPlan:
         self.window = window
         self.pad_mode = int(pad_mode)
         self.bins = self.n_fft // 2 + 1
+        self.phase_budget = int(phase_budget)
         if window not in WINDOWS:
             raise ValueError(f"unknown window {window!r}")
         self.device = torch.cuda.current_device() if device is None else int(device)
@@ -94,6 +103,48 @@ class StftPlan:
             raise RuntimeError(f"fftfree_stft_magnitude returned {got} frames, expected {F}")
         return out[0] if x.dim() == 1 else out
 
+    def stores_phase(self, x: torch.Tensor) -> bool:
+        """True when the forward pass of ``x`` saves the unit phasor X / |X|
+        for the backward (its size within ``phase_budget``) rather than
+        leaving the spectrum to be recomputed."""
+        S = 1 if x.dim() == 1 else x.shape[0]
+        return S * self.frames(x.shape[-1]) * self.bins * 8 <= self.phase_budget
+
+    def magnitude_phasor(self, x: torch.Tensor) -> Tuple[torch.Tensor, torch.Tensor]:
+        """(|STFT|, STFT / |STFT|) with the layout of ``magnitude``, the
+        phasor complex64 and 0 where |X| = 0."""
+        x = self._check(x)
+        x2 = x.view(1, -1) if x.dim() == 1 else x
+        S, L = x2.shape
+        F = self.frames(L)
+        if F == 0:
+            raise ValueError("signal shorter than one frame")
+        mag = torch.empty((S, F, self.bins), dtype=torch.float32, device=x.device)
+        ph = torch.empty((S, F, self.bins), dtype=torch.complex64, device=x.device)
+        self._bind_stream()
+        got = self.ctx.stft_magnitude_phasor(x2, S, L, mag, ph)
+        if got != F:
+            raise RuntimeError(f"fftfree_stft_magnitude_phasor returned {got} frames, expected {F}")
+        return (mag[0], ph[0]) if x.dim() == 1 else (mag, ph)
+
+    def magnitude_backward_phasor(self, phasor: torch.Tensor, grad_mag: torch.Tensor, length: int) -> torch.Tensor:
+        """d(sum(grad_mag * |STFT x|))/dx from the phasor ``magnitude_phasor``
+        saved; (signals, length), or (length,) for a 2-D phasor."""
+        ph = phasor.contiguous()
+        if ph.dtype != torch.complex64:
+            raise TypeError("phasor must be complex64")
+        S = 1 if ph.dim() == 2 else ph.shape[0]
+        F = self.frames(length)
+        g = grad_mag.to(dtype=torch.float32).contiguous()
+        if ph.numel() != S * F * self.bins or g.numel() != ph.numel() or not g.is_cuda or not ph.is_cuda:
+            raise ValueError("phasor / grad_mag do not match the forward output")
+        gx = torch.empty((S, length), dtype=torch.float32, device=ph.device)
+        self._bind_stream()
+        got = self.ctx.stft_magnitude_backward_phasor(ph, S, length, g, gx)
+        if got != F:
+            raise RuntimeError(f"fftfree_stft_magnitude_backward_phasor returned {got} frames, expected {F}")
+        return gx[0] if ph.dim() == 2 else gx
+
     def magnitude_backward(self, x: torch.Tensor, grad_mag: torch.Tensor) -> torch.Tensor:
         """d(sum(grad_mag * |STFT x|))/dx, shaped like x."""
         x = self._check(x)
@@ -119,15 +170,23 @@ class StftPlan:
 class _StftMagnitude(torch.autograd.Function):
     @staticmethod
     def forward(ctx, x: torch.Tensor, plan: StftPlan) -> torch.Tensor:
-        mag = plan.magnitude(x)
-        ctx.save_for_backward(x)  # the spectrum is recomputed, not stored
         ctx.plan = plan
+        ctx.length = x.shape[-1]
+        ctx.with_phase = plan.stores_phase(x)
+        if ctx.with_phase:
+            mag, ph = plan.magnitude_phasor(x)
+            ctx.save_for_backward(ph)
+        else:
+            mag = plan.magnitude(x)
+            ctx.save_for_backward(x)  # long signals: the spectrum is recomputed, not stored
         return mag
 
     @staticmethod
     def backward(ctx, grad_mag: torch.Tensor):
-        (x,) = ctx.saved_tensors
-        return ctx.plan.magnitude_backward(x, grad_mag), None
+        (saved,) = ctx.saved_tensors
+        if ctx.with_phase:
+            return ctx.plan.magnitude_backward_phasor(saved, grad_mag, ctx.length), None
+        return ctx.plan.magnitude_backward(saved, grad_mag), None
 
 
 def stft_magnitude(x: torch.Tensor, plan: StftPlan) -> torch.Tensor:

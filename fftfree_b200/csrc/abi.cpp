@@ -961,23 +961,36 @@ static int mag_grad_span(int H) {
   return (int)s;
 }
 
-FFT_CFFI_API size_t fftfree_stft_magnitude(void* handle, const float* pcm, size_t signals, size_t length,
-                                           float* out_mag, size_t max_frames) {
+static int mag_grad_run() {
+  static const int env = [] {
+    const char* e = std::getenv("FFTFREE_GRAD_RUN");
+    return e ? std::atoi(e) : -1;
+  }();
+  return env >= 0 ? env : 32;  // frames per thread group; 0 selects the general form
+}
+
+// Shared body of the magnitude STFT entry points; out_phasor (X / |X| as
+// interleaved pairs, 0 where |X| = 0) is written when not null.
+static size_t stft_magnitude(void* handle, const float* pcm, size_t signals, size_t length, float* out_mag,
+                             float* out_phasor, size_t max_frames, const char* who) {
   FftContext* c = as_ctx(handle);
   if (!c || !pcm || !out_mag || signals == 0 || length == 0) return 0;
   try {
     std::lock_guard<std::recursive_mutex> lk(c->mu);
-    if (!mag_grad_ctx_ok(c, "fftfree_stft_magnitude")) return 0;
+    if (!mag_grad_ctx_ok(c, who)) return 0;
     DeviceGuard g(c->device);
     const size_t frames = frame_count(c, length, 0, max_frames);
     if (frames == 0) return 0;
     const int W = c->window ? c->window : c->N;
     const int H = c->hop ? c->hop : W;
     const int bins = c->N / 2 + 1;
+    const size_t outn = signals * frames * (size_t)bins;
     bool any_host = !is_device_ptr(pcm);
     const float* d_pcm = stage_in(c, c->d_in0, pcm, signals * length);
-    OutTarget o = stage_out(c->d_out2, out_mag, signals * frames * (size_t)bins);
-    any_host = any_host || o.host;
+    OutTarget o = stage_out(c->d_out2, out_mag, outn);
+    OutTarget op;
+    if (out_phasor) op = stage_out(c->d_out1, out_phasor, 2 * outn);
+    any_host = any_host || o.host || op.host;
     StftArgs a{};
     a.pcm = d_pcm;
     a.pcm_len = (long long)length;
@@ -990,11 +1003,13 @@ FFT_CFFI_API size_t fftfree_stft_magnitude(void* handle, const float* pcm, size_
     a.out_bins = bins;
     a.out_stride = bins;
     a.out_mag = o.dev;
+    a.out_phasor = out_phasor ? reinterpret_cast<float2*>(op.dev) : nullptr;
     a.sig_frames = (long long)frames;
     a.sig_stride = (long long)length;
-    a.mag_only = 1;
+    a.mag_only = out_phasor ? 2 : 1;
     FFB_CHECK(launch_stft(a, c->logr_req, c->stream, &c->launches));
     finish_out(c, o);
+    if (out_phasor) finish_out(c, op);
     finish_call(c, any_host);
     return frames;
   } catch (...) {
@@ -1002,26 +1017,50 @@ FFT_CFFI_API size_t fftfree_stft_magnitude(void* handle, const float* pcm, size_
   }
 }
 
-FFT_CFFI_API size_t fftfree_stft_magnitude_backward(void* handle, const float* pcm, size_t signals,
-                                                    size_t length, const float* grad_mag, float* grad_pcm) {
+FFT_CFFI_API size_t fftfree_stft_magnitude(void* handle, const float* pcm, size_t signals, size_t length,
+                                           float* out_mag, size_t max_frames) {
+  return stft_magnitude(handle, pcm, signals, length, out_mag, nullptr, max_frames, "fftfree_stft_magnitude");
+}
+
+FFT_CFFI_API size_t fftfree_stft_magnitude_phasor(void* handle, const float* pcm, size_t signals, size_t length,
+                                                  float* out_mag, float* out_phasor, size_t max_frames) {
+  if (!out_phasor) return 0;
+  return stft_magnitude(handle, pcm, signals, length, out_mag, out_phasor, max_frames,
+                        "fftfree_stft_magnitude_phasor");
+}
+
+// Shared body of the gradient entry points: the spectrum comes from pcm
+// (recomputed) or from a saved unit phasor.
+static size_t stft_magnitude_backward(void* handle, const float* pcm, const float* phasor, size_t signals,
+                                      size_t length, const float* grad_mag, float* grad_pcm, const char* who) {
   FftContext* c = as_ctx(handle);
-  if (!c || !pcm || !grad_mag || !grad_pcm || signals == 0 || length == 0) return 0;
+  if (!c || !(pcm || phasor) || !grad_mag || !grad_pcm || signals == 0 || length == 0) return 0;
   try {
     std::lock_guard<std::recursive_mutex> lk(c->mu);
-    if (!mag_grad_ctx_ok(c, "fftfree_stft_magnitude_backward")) return 0;
+    if (!mag_grad_ctx_ok(c, who)) return 0;
     DeviceGuard g(c->device);
     const size_t frames = frame_count(c, length, 0, 0);
     if (frames == 0) return 0;
     const int W = c->window ? c->window : c->N;
     const int H = c->hop ? c->hop : W;
     const int bins = c->N / 2 + 1;
-    bool any_host = !is_device_ptr(pcm) || !is_device_ptr(grad_mag);
-    const float* d_pcm = stage_in(c, c->d_in0, pcm, signals * length);
-    const float* d_g = stage_in(c, c->d_in1, grad_mag, signals * frames * (size_t)bins);
+    const size_t specn = signals * frames * (size_t)bins;
+    bool any_host = !is_device_ptr(grad_mag);
+    const float* d_pcm = nullptr;
+    const float* d_ph = nullptr;
+    if (phasor) {
+      any_host = any_host || !is_device_ptr(phasor);
+      d_ph = stage_in(c, c->d_in0, phasor, 2 * specn);
+    } else {
+      any_host = any_host || !is_device_ptr(pcm);
+      d_pcm = stage_in(c, c->d_in0, pcm, signals * length);
+    }
+    const float* d_g = stage_in(c, c->d_in1, grad_mag, specn);
     OutTarget o = stage_out(c->d_out0, grad_pcm, signals * length);
     any_host = any_host || o.host;
     MagGradArgs a{};
     a.pcm = d_pcm;
+    a.phasor = reinterpret_cast<const float2*>(d_ph);
     a.signals = (long long)signals;
     a.pcm_len = (long long)length;
     a.sig_stride = (long long)length;
@@ -1033,6 +1072,7 @@ FFT_CFFI_API size_t fftfree_stft_magnitude_backward(void* handle, const float* p
     a.grad_mag = d_g;
     a.grad_pcm = o.dev;
     a.span = mag_grad_span(H);
+    a.run = mag_grad_run();
     FFB_CHECK(launch_stft_mag_grad(a, c->logr_req, c->stream, &c->launches));
     finish_out(c, o);
     finish_call(c, any_host);
@@ -1040,6 +1080,21 @@ FFT_CFFI_API size_t fftfree_stft_magnitude_backward(void* handle, const float* p
   } catch (...) {
     return 0;
   }
+}
+
+FFT_CFFI_API size_t fftfree_stft_magnitude_backward(void* handle, const float* pcm, size_t signals,
+                                                    size_t length, const float* grad_mag, float* grad_pcm) {
+  if (!pcm) return 0;
+  return stft_magnitude_backward(handle, pcm, nullptr, signals, length, grad_mag, grad_pcm,
+                                 "fftfree_stft_magnitude_backward");
+}
+
+FFT_CFFI_API size_t fftfree_stft_magnitude_backward_phasor(void* handle, const float* phasor, size_t signals,
+                                                           size_t length, const float* grad_mag,
+                                                           float* grad_pcm) {
+  if (!phasor) return 0;
+  return stft_magnitude_backward(handle, nullptr, phasor, signals, length, grad_mag, grad_pcm,
+                                 "fftfree_stft_magnitude_backward_phasor");
 }
 
 FFT_CFFI_API void fftfree_set_stream(void* handle, void* cuda_stream) {

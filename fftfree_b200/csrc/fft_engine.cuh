@@ -58,7 +58,7 @@ __host__ __device__ constexpr long long pass_table_offset(int lr, int lns) {
   for (int l = 1; l < lr; ++l) off += (long long)((1 << l) - 1) * ((1LL << (kPassMaxLog + 1)) - 1);
   return off + (long long)((1 << lr) - 1) * ((1LL << lns) - 1);
 }
-constexpr long long pass_table_size() { return pass_table_offset(5, 0); }
+constexpr long long pass_table_size() { return pass_table_offset(6, 0); }  // radices 2..32
 
 struct Twiddles {
   const float2* __restrict__ pyr;
@@ -91,6 +91,25 @@ __device__ __forceinline__ float2 w16(int m) {
     case 13: return make_float2(s1, c1);
     case 14: return make_float2(h, h);
     default: return make_float2(c1, s1);
+  }
+}
+
+// exp(-2*pi*i*m/32), 0 <= m < 16
+__device__ __forceinline__ float2 w32(int m) {
+  constexpr float c1 = 0.98078528040323044913f;  // cos(pi/16)
+  constexpr float s1 = 0.19509032201612826785f;  // sin(pi/16)
+  constexpr float c3 = 0.83146961230254523708f;  // cos(3pi/16)
+  constexpr float s3 = 0.55557023301960222474f;  // sin(3pi/16)
+  switch (m) {
+    case 1: return make_float2(c1, -s1);
+    case 3: return make_float2(c3, -s3);
+    case 5: return make_float2(s3, -c3);
+    case 7: return make_float2(s1, -c1);
+    case 9: return make_float2(-s1, -c1);
+    case 11: return make_float2(-s3, -c3);
+    case 13: return make_float2(-c3, -s3);
+    case 15: return make_float2(-c1, -s1);
+    default: return w16(m >> 1);
   }
 }
 
@@ -184,6 +203,27 @@ struct Dft<16> {
   }
 };
 
+template <>
+struct Dft<32> {
+  __device__ __forceinline__ static void run(float2* v) {
+    // 2 x 16: X[k] = E[k] + w32^k O[k], X[k + 16] = E[k] - w32^k O[k]
+    float2 e[16], o[16];
+#pragma unroll
+    for (int n = 0; n < 16; ++n) {
+      e[n] = v[2 * n];
+      o[n] = v[2 * n + 1];
+    }
+    Dft<16>::run(e);
+    Dft<16>::run(o);
+#pragma unroll
+    for (int k = 0; k < 16; ++k) {
+      const float2 t = (k == 0) ? o[0] : (k == 8 ? mul_mi(o[8]) : cmul(o[k], w32(k)));
+      v[k] = cadd(e[k], t);
+      v[k + 16] = csub(e[k], t);
+    }
+  }
+};
+
 // ---------------------------------------------------------------- schedule
 template <int LOGM_, int LOGR_>
 struct Sched {
@@ -195,6 +235,33 @@ struct Sched {
   static constexpr int NFULL = (LOGR > 0) ? LOGM / LOGR : 0;   // full radix-R passes
   static constexpr int LOGR0 = (LOGR > 0) ? LOGM % LOGR : 0;   // leading small pass
   static constexpr int SMEM = M + (M >> 4) + 2;                // padded tile (float2), index M included
+};
+
+// Barrier policies of the engine.  BlockSync: the whole block (kernels
+// whose blocks share tiles across transforms).  GroupSync: only the S::T
+// threads of one transform -- a warp barrier when a transform fits in a
+// warp, else a named barrier per group of a block of 256 threads (groups
+// are the consecutive S::T-thread slices; at most 4 of them here), or the
+// block barrier when one transform is the whole block.
+struct BlockSync {
+  template <class S>
+  __device__ __forceinline__ static void sync() {
+    __syncthreads();
+  }
+};
+
+struct GroupSync {
+  template <class S>
+  __device__ __forceinline__ static void sync() {
+    if constexpr (S::T <= 32) {
+      __syncwarp();
+    } else if constexpr (S::T >= 256) {
+      __syncthreads();
+    } else {
+      static_assert(256 / S::T <= 15, "one named barrier per group");
+      asm volatile("bar.sync %0, %1;" ::"r"(1 + (int)(threadIdx.x / S::T)), "n"(S::T) : "memory");
+    }
+  }
 };
 
 // Padded shared-memory index: one float2 of padding per 16.
@@ -226,7 +293,7 @@ __device__ __forceinline__ void tile_write_natural(const float2 (&v)[S::R], int 
   }
 }
 
-template <class S, int P>
+template <class S, class Y, int P>
 __device__ __forceinline__ void stockham_pass(float2 (&v)[S::R], int t, float2* sm, const Twiddles& tw) {
   constexpr int R = S::R, LR = S::LOGR;
   constexpr int LNS = S::LOGR0 + P * LR;
@@ -249,21 +316,21 @@ __device__ __forceinline__ void stockham_pass(float2 (&v)[S::R], int t, float2* 
 #pragma unroll
       for (int r = 0; r < R; ++r) sm[pidx(base + r * NS)] = v[r];
     }
-    __syncthreads();
+    Y::template sync<S>();
     tile_read<S>(v, t, sm);
-    __syncthreads();
+    Y::template sync<S>();
   }
 }
 
-template <class S, int... P>
+template <class S, class Y, int... P>
 __device__ __forceinline__ void run_passes(float2 (&v)[S::R], int t, float2* sm, const Twiddles& tw,
                                            std::integer_sequence<int, P...>) {
-  (stockham_pass<S, P>(v, t, sm, tw), ...);
+  (stockham_pass<S, Y, P>(v, t, sm, tw), ...);
 }
 
 // The engine.  `sm` is this group's padded tile (S::SMEM float2); every
-// thread of the block calls the engine (it contains block barriers).
-template <class S>
+// thread of the block (BlockSync) or of the group (GroupSync) calls it.
+template <class S, class Y = BlockSync>
 __device__ __forceinline__ void fft_engine(float2 (&v)[S::R], int t, float2* sm, const Twiddles& tw) {
   constexpr int R = S::R, T = S::T;
   if constexpr (S::LOGR0 > 0) {
@@ -279,11 +346,11 @@ __device__ __forceinline__ void fft_engine(float2 (&v)[S::R], int t, float2* sm,
 #pragma unroll
       for (int r = 0; r < r0; ++r) sm[pidx(j * r0 + r)] = u[r];
     }
-    __syncthreads();
+    Y::template sync<S>();
     tile_read<S>(v, t, sm);
-    __syncthreads();
+    Y::template sync<S>();
   }
-  run_passes<S>(v, t, sm, tw, std::make_integer_sequence<int, S::NFULL>{});
+  run_passes<S, Y>(v, t, sm, tw, std::make_integer_sequence<int, S::NFULL>{});
 }
 
 }  // namespace ffb

@@ -24,7 +24,7 @@ k_fft(IO io, Twiddles tw) {
   float2* sm = smem + g * S::SMEM;
   float2 v[S::R];
   io.template load<S>(b, t, v, sm, tw);
-  fft_engine<S>(v, t, sm, tw);
+  fft_engine<S, GroupSync>(v, t, sm, tw);
   io.template store<S>(b, t, v, sm, tw);
 }
 
@@ -47,7 +47,7 @@ static cudaError_t run(const IO& io, long long nbatch, cudaStream_t st, uint64_t
 }
 
 // Compile-time table of instantiations: LOGM 0..13, LOGR 2..4 (clamped by
-// Sched), threads per transform <= 1024.
+// Sched) and 5 from LOGM 9 up, threads per transform <= 1024.
 template <class IO, int LOGM, int LOGR>
 static cudaError_t run_if_valid(const IO& io, long long n, cudaStream_t st, uint64_t* l) {
   using S = Sched<LOGM, LOGR>;
@@ -63,6 +63,9 @@ static cudaError_t dispatch_r(const IO& io, int logr, long long n, cudaStream_t 
   switch (logr) {
     case 2: return run_if_valid<IO, LOGM, 2>(io, n, st, l);
     case 3: return run_if_valid<IO, LOGM, 3>(io, n, st, l);
+    case 5:
+      if constexpr (LOGM >= 9) return run_if_valid<IO, LOGM, 5>(io, n, st, l);
+      else return run_if_valid<IO, LOGM, 4>(io, n, st, l);
     default: return run_if_valid<IO, LOGM, 4>(io, n, st, l);
   }
 }

@@ -70,6 +70,14 @@ __device__ __forceinline__ float2 post_hook_m(float2 X, int k, int N, const Post
 
 __host__ __device__ inline int post_mode(const PostFlags& pf) { return pf.polar ? 2 : (pf.reduce ? 1 : 0); }
 
+// X / |X| for the magnitude gradient's saved phasor; 0 where |X| = 0, where
+// the gradient of |X| is taken as 0.
+__device__ __forceinline__ float2 unit_phasor(float2 X, float mag) {
+  if (!(mag > 0.f)) return make_float2(0.f, 0.f);
+  const float r = 1.0f / mag;
+  return make_float2(X.x * r, X.y * r);
+}
+
 // Frame f of a (possibly multi-signal) STFT: its first sample and how many
 // samples it takes from the signal (fft_cffi.cpp:765-791: frame f covers
 // pcm[f*H .. f*H + W), zero beyond the signal end and from W up to N).
@@ -90,7 +98,8 @@ __device__ __forceinline__ const float* stft_frame(const float* pcm, long long p
 
 // ------------------------------------------------------------------ STFT IO
 // MODE: 0 plain / imag clear, 1 reduce_magnitude, 2 store_polar, 3 |X| only
-// (forward half spectrum, magnitude array alone).
+// (forward half spectrum, magnitude array alone), 4 |X| into the magnitude
+// array and the unit phasor X / |X| into out_phasor (0 where |X| = 0).
 template <int MODE>
 struct StftIO {
   StftArgs a;
@@ -163,7 +172,8 @@ struct StftIO {
     if (f >= a.frames || k >= a.out_bins) return;
     const long long ob = f * a.out_stride;
     const bool mag_is_re = (MODE == 1) || (MODE == 2 && a.mag_from_real);
-    emit(a.out_re + (MODE == 3 ? 0 : ob), a.out_im + (MODE == 3 ? 0 : ob), a.out_mag + ob, (int)k, X,
+    emit(MODE == 4 ? reinterpret_cast<float*>(a.out_phasor + ob) : a.out_re + (MODE == 3 ? 0 : ob),
+         a.out_im + (MODE >= 3 ? 0 : ob), a.out_mag + ob, (int)k, X,
          k == 0 || 2 * k == a.N, 1.0f / (float)a.N, mag_is_re);
   }
 
@@ -175,8 +185,10 @@ struct StftIO {
     // Real input: DC and Nyquist are exactly real (imag +0), as in the
     // reference's radix-2 executors.
     if (dc_or_nyq) X.y = 0.f;
-    if constexpr (MODE == 3) {
-      mg[k] = cabs_fast(X.x, X.y);
+    if constexpr (MODE >= 3) {
+      const float m = cabs_fast(X.x, X.y);
+      mg[k] = m;
+      if constexpr (MODE == 4) reinterpret_cast<float2*>(re)[k] = unit_phasor(X, m);  // re: phasor row
       return;
     }
     X = post_hook_m<MODE>(X, k, a.N, a.pf);
@@ -190,11 +202,11 @@ struct StftIO {
                                         const Twiddles& tw) const {
     constexpr int M = S::M, T = S::T, R = S::R;
     tile_write_natural<S>(v, t, sm);
-    __syncthreads();
+    GroupSync::sync<S>();
     if (f >= a.frames) return;
     const long long ob = f * a.out_stride;
-    float* re = a.out_re + (MODE == 3 ? 0 : ob);
-    float* im = a.out_im + (MODE == 3 ? 0 : ob);
+    float* re = (MODE == 4) ? reinterpret_cast<float*>(a.out_phasor + ob) : a.out_re + (MODE == 3 ? 0 : ob);
+    float* im = a.out_im + (MODE >= 3 ? 0 : ob);
     float* mg = a.out_mag + ob;
     const bool mag_is_re = (MODE == 1) || (MODE == 2 && a.mag_from_real);
     if (a.N == 1) {
@@ -220,8 +232,10 @@ struct StftIO {
         const float2 O = make_float2(0.5f * D.y, -0.5f * D.x);
         float2 X = cadd(E, cmul(__ldg(w + i * T), O));
         if (i == 0 && t == 0) X.y = 0.f;  // DC
-        if constexpr (MODE == 3) {
-          pm[i * T] = cabs_fast(X.x, X.y);
+        if constexpr (MODE >= 3) {
+          const float m = cabs_fast(X.x, X.y);
+          pm[i * T] = m;
+          if constexpr (MODE == 4) reinterpret_cast<float2*>(re)[t + i * T] = unit_phasor(X, m);
           continue;
         }
         float mag;
@@ -451,7 +465,7 @@ struct C2rHalfIO {
       }
       if (t == 0) sm[pidx(M)] = bin(re, im, M, true, cs);
     }
-    __syncthreads();
+    GroupSync::sync<S>();
     const float2* w = tw.pyr + ((1 << LN) - 1) + t;
 #pragma unroll
     for (int i = 0; i < R; ++i) {
@@ -466,7 +480,7 @@ struct C2rHalfIO {
       }
       v[i] = cconj(z);  // IDFT via conj . DFT . conj
     }
-    __syncthreads();  // the engine reuses the tile
+    GroupSync::sync<S>();  // the engine reuses the tile
   }
 
   template <class S>

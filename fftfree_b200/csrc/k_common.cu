@@ -1,5 +1,6 @@
 // k_common.cu -- schedule choice, overlap-add gather and the twiddle tables.
 #include <cmath>
+#include <cstdlib>
 #include <mutex>
 #include <vector>
 
@@ -9,16 +10,41 @@ namespace ffb {
 
 int max_single_pass_log() { return 13; }
 
+// Radix 32 passes are instantiated for transforms of 2^9 points and up.
+constexpr int kMinLogmRadix32 = 9;
+
+static int env_logr(const char* name) {
+  const char* e = std::getenv(name);
+  return e ? std::atoi(e) : 0;
+}
+
 int choose_logr(int logm, int requested_log, bool real_path) {
   if (logm > max_single_pass_log()) return -1;
-  auto valid = [&](int lr) { return lr >= 2 && lr <= 4 && (logm - (lr < logm ? lr : logm)) <= 10; };
-  if (requested_log >= 2 && requested_log <= 4 && valid(requested_log)) return requested_log;
-  // Default schedule, from B200 sweeps: complex transforms radix 16 from
-  // 1024 points up, 8 below; the real-input paths (which add an untangle
-  // step per bin) radix 8 up to 4096 points.
+  auto valid = [&](int lr) {
+    if (lr == 5) return logm >= kMinLogmRadix32 && logm - 5 <= 10;
+    return lr >= 2 && lr <= 4 && (logm - (lr < logm ? lr : logm)) <= 10;
+  };
+  // FFTFREE_DEFAULT_LOGR_REAL / _COMPLEX override the default (sweeps)
+  static const int env_real = env_logr("FFTFREE_DEFAULT_LOGR_REAL");
+  static const int env_cplx = env_logr("FFTFREE_DEFAULT_LOGR_COMPLEX");
+  const int env = real_path ? env_real : env_cplx;
+  if (env >= 2 && env <= 5 && valid(env)) return env;
+  // Default schedule, from B200 sweeps (one-warp transforms sync with warp
+  // barriers, larger ones with a named barrier per transform): complex
+  // transforms radix 32 at 1024 and 8192 points (a single exchange, or two
+  // on 256 threads), radix 16 at 256..512 and 2048..4096, radix 8 below;
+  // the real-input paths (an N/2-point transform plus the untangle) radix 16
+  // at 512..1024 and 8192 complex points, radix 8 otherwise.
   int lr;
-  if (real_path) lr = (logm >= 13) ? 4 : (logm >= 6 ? 3 : 2);
-  else lr = (logm >= 10) ? 4 : (logm >= 6 ? 3 : 2);
+  if (real_path) lr = (logm == 9 || logm == 10 || logm >= 13) ? 4 : (logm >= 6 ? 3 : 2);
+  else if (logm == 10 || logm == 13) lr = 5;
+  else lr = (logm >= 8) ? 4 : (logm >= 6 ? 3 : 2);
+  // The plan's radix option / pattern (radix 4, 8 or 16; fft_cffi.hpp:67-72)
+  // is a lower bound on the pass radix.  The reference's Stockham executor
+  // runs radix-2 stages whatever it names (plan_support.hpp:136-150 only
+  // selects an enum), so it fixes no result beyond rounding; a smaller
+  // radix than the default only adds exchange passes on the GPU.
+  if (requested_log >= 2 && requested_log <= 4 && requested_log > lr && valid(requested_log)) lr = requested_log;
   while (!valid(lr) && lr < 4) ++lr;
   return valid(lr) ? lr : -1;
 }
@@ -159,7 +185,7 @@ const float2* twiddle_pass_tables(cudaStream_t stream) {
   if (g_pass[dev]) return g_pass[dev];
   const long long total = pass_table_size();
   std::vector<float2> host((size_t)total);
-  for (int lr = 1; lr <= 4; ++lr) {
+  for (int lr = 1; lr <= 5; ++lr) {
     const int R = 1 << lr;
     for (int lns = 0; lns <= kPassMaxLog; ++lns) {
       const long long Ns = 1LL << lns;

@@ -17,6 +17,8 @@
 // are transformed by both neighbours); the overlap-add adjoint is a gather
 // in frame order through a shared-memory accumulator, so the result is
 // deterministic and needs no atomics.
+#include <cstdlib>
+
 #include "fft_launch.cuh"
 
 namespace ffb {
@@ -32,6 +34,9 @@ cudaError_t with_r(int logr, F&& f) {
   switch (logr) {
     case 2: return f(SchedTag<Sched<LOGM, 2>>{});
     case 3: return f(SchedTag<Sched<LOGM, 3>>{});
+    case 5:
+      if constexpr (LOGM >= 9) return f(SchedTag<Sched<LOGM, 5>>{});
+      else return f(SchedTag<Sched<LOGM, 4>>{});
     default: return f(SchedTag<Sched<LOGM, 4>>{});
   }
 }
@@ -99,12 +104,155 @@ __device__ __forceinline__ float2 mag_chain(float2 X, float g) {
   return make_float2(X.x * s, X.y * s);
 }
 
+// Blocks per SM the register budget is sized for: the kernel holds a frame
+// and its gradient spectrum in registers; capping registers at 64 (radix 8)
+// or 80 (radix 16) keeps enough warps resident to hide the load latency.
 template <class S>
-__global__ void __launch_bounds__(Launch<S>::BLOCK) k_stft_mag_grad(MagGradArgs a, Twiddles tw) {
+constexpr int grad_min_blocks() {
+  constexpr int want = S::R <= 8 ? 4 : (S::R == 16 ? 3 : 1);
+  constexpr int fit64 = 65536 / (Launch<S>::BLOCK * 64);  // blocks at 64 registers a thread
+  return want < fit64 ? want : (fit64 > 1 ? fit64 : 1);
+}
+
+// Hermitian half spectrum y (bins t + i*T, the Nyquist bin in ynyq on
+// thread 0; DC and Nyquist already doubled) to the windowed frame gradient:
+// v[i] holds samples n = 2m, 2m+1 (m = t + i*T) of w[n] dL/ds[n], zero from
+// `cnt` on.  The tile must be free on entry; it is free on return.
+template <class S>
+__device__ __forceinline__ void grad_inverse(const MagGradArgs& a, const float2 (&y)[S::R], float2 ynyq,
+                                             long long cnt, int t, float2* sm, const Twiddles& tw,
+                                             float2 (&v)[S::R]) {
+  constexpr int T = S::T, R = S::R, M = S::M;
+  constexpr int LN = S::LOGM + 1;  // N = 2M
+  const float2* w = tw.pyr + ((1 << LN) - 1) + t;  // e^{-2 pi i m / N}, m = t + i*T
+  tile_write_natural<S>(y, t, sm);
+  if (t == 0) sm[pidx(M)] = ynyq;
+  GroupSync::sync<S>();
+
+  // Hermitian half spectrum Y -> z' with x[2m] = Re, x[2m+1] = Im of the
+  // unnormalised inverse: E = (Y[m] + conj Y[M-m]) / 2,
+  // O = (Y[m] - conj Y[M-m]) e^{+2 pi i m/N} / 2, z' = IDFT_M(E + i O),
+  // the IDFT taken as conj . DFT . conj.
+#pragma unroll
+  for (int i = 0; i < R; ++i) {
+    const int m = t + i * T;
+    const float2 ym = sm[pidx(M - m)];
+    const float2 E = make_float2(0.5f * (y[i].x + ym.x), 0.5f * (y[i].y - ym.y));
+    const float2 D = make_float2(0.5f * (y[i].x - ym.x), 0.5f * (y[i].y + ym.y));
+    const float2 O = cmul(D, cconj(__ldg(w + i * T)));
+    v[i] = make_float2(E.x - O.y, -(E.y + O.x));
+  }
+  GroupSync::sync<S>();  // the engine reuses the tile
+  fft_engine<S, GroupSync>(v, t, sm, tw);
+
+  // dL/ds[2m] = Re, dL/ds[2m+1] = -Im, times the window, zero past the frame's samples.
+#pragma unroll
+  for (int i = 0; i < R; ++i) {
+    const int n = 2 * (t + i * T);
+    float d0 = v[i].x, d1 = -v[i].y;
+    if (a.win) {
+      d0 *= __ldg(a.win + n);
+      d1 *= __ldg(a.win + n + 1);
+    }
+    if (n >= cnt) d0 = 0.f;
+    if (n + 1 >= cnt) d1 = 0.f;
+    v[i] = make_float2(d0, d1);
+  }
+}
+
+// One frame's gradient dL/ds, windowed: on return v[i] holds the samples
+// n = 2m, 2m + 1 (m = t + i*T) of w[n] dL/ds_f[n], zero from the frame's
+// sample count on.  Every group barrier is inside; the tile is free on
+// return (its last reads are behind a barrier).
+template <class S>
+__device__ __forceinline__ void frame_grad(const MagGradArgs& a, const float* pcm, const float* gsig, long long f,
+                                           bool ok, int t, float2* sm, const Twiddles& tw, float2 (&v)[S::R]) {
+  constexpr int T = S::T, R = S::R, M = S::M;
+  constexpr int LN = S::LOGM + 1;  // N = 2M
+  const float2* w = tw.pyr + ((1 << LN) - 1) + t;  // e^{-2 pi i k / N}, k = t + i*T
+  long long cnt;
+  grad_load<S>(a, pcm, f, ok, t, v, &cnt);
+  // upstream gradient of this frame's bins, fetched before the transform
+  const float* gf = gsig + (ok ? f : 0) * (long long)(M + 1);
+  float gk[R];
+#pragma unroll
+  for (int i = 0; i < R; ++i) gk[i] = ok ? __ldg(gf + t + i * T) : 0.f;
+  fft_engine<S, GroupSync>(v, t, sm, tw);
+
+  // Untangle Z (the M-point transform of z) into X[k], k = t + i*T, and
+  // apply the magnitude chain rule bin by bin.
+  tile_write_natural<S>(v, t, sm);
+  GroupSync::sync<S>();
+  float2 y[R];
+#pragma unroll
+  for (int i = 0; i < R; ++i) {
+    const int k = t + i * T;
+    const float2 zk = v[i];
+    const float2 zm = sm[pidx((M - k) & (M - 1))];
+    const float2 E = make_float2(0.5f * (zk.x + zm.x), 0.5f * (zk.y - zm.y));
+    const float2 D = make_float2(zk.x - zm.x, zk.y + zm.y);
+    const float2 O = make_float2(0.5f * D.y, -0.5f * D.x);
+    float2 X = cadd(E, cmul(__ldg(w + i * T), O));
+    if (i == 0 && t == 0) {
+      X.y = 0.f;  // DC is real
+      const float2 V = mag_chain(X, gk[0]);
+      y[i] = make_float2(2.f * V.x, 0.f);
+    } else {
+      y[i] = mag_chain(X, gk[i]);
+    }
+  }
+  float2 ynyq = make_float2(0.f, 0.f);
+  if (t == 0) {  // Nyquist X[M] = Re Z[0] - Im Z[0]
+    const float xn = v[0].x - v[0].y;
+    const float gn = ok ? __ldg(gf + M) : 0.f;
+    ynyq = make_float2(2.f * mag_chain(make_float2(xn, 0.f), gn).x, 0.f);
+  }
+  GroupSync::sync<S>();  // every read of Z is done
+  grad_inverse<S>(a, y, ynyq, cnt, t, sm, tw, v);
+}
+
+// The same from the unit phasor U = X / |X| the forward pass saved:
+// V = g U -- no forward transform, no signal read.
+template <class S>
+__device__ __forceinline__ void frame_grad_phasor(const MagGradArgs& a, const float* gsig, const float2* usig,
+                                                  long long f, bool ok, int t, float2* sm, const Twiddles& tw,
+                                                  float2 (&v)[S::R]) {
+  constexpr int T = S::T, R = S::R, M = S::M;
+  long long cnt = 0;
+  if (ok) {
+    cnt = a.pcm_len - f * (long long)a.H;
+    if (cnt > a.W) cnt = a.W;
+  }
+  const long long off = (ok ? f : 0) * (long long)(M + 1);
+  float2 y[R];
+#pragma unroll
+  for (int i = 0; i < R; ++i) {
+    const int k = t + i * T;
+    float2 V = make_float2(0.f, 0.f);
+    if (ok) V = cscale(__ldg(usig + off + k), __ldg(gsig + off + k));
+    y[i] = (i == 0 && t == 0) ? make_float2(2.f * V.x, 0.f) : V;  // DC is real
+  }
+  float2 ynyq = make_float2(0.f, 0.f);
+  if (t == 0 && ok) ynyq = make_float2(2.f * __ldg(gsig + off + M) * __ldg(usig + off + M).x, 0.f);  // Nyquist
+  grad_inverse<S>(a, y, ynyq, cnt, t, sm, tw, v);
+}
+
+template <class S, bool PH>
+__device__ __forceinline__ void frame_grad_any(const MagGradArgs& a, const float* pcm, const float2* psig,
+                                               const float* gsig, long long f, bool ok, int t, float2* sm,
+                                               const Twiddles& tw, float2 (&v)[S::R]) {
+  if constexpr (PH) frame_grad_phasor<S>(a, gsig, psig, f, ok, t, sm, tw, v);
+  else frame_grad<S>(a, pcm, gsig, f, ok, t, sm, tw, v);
+}
+
+// General form: each block owns `span` samples of one signal and gathers
+// the frames that touch them through a shared-memory accumulator.
+template <class S, bool PH>
+__global__ void __launch_bounds__(Launch<S>::BLOCK, grad_min_blocks<S>()) k_stft_mag_grad(MagGradArgs a,
+                                                                                          Twiddles tw) {
   extern __shared__ float2 smem[];
   constexpr int T = S::T, R = S::R, M = S::M;
   constexpr int G = Launch<S>::G, B = Launch<S>::BLOCK;
-  constexpr int LN = S::LOGM + 1;  // N = 2M
   const int g = threadIdx.x / T;
   const int t = threadIdx.x - g * T;
   float2* sm = smem + g * S::SMEM;
@@ -121,85 +269,17 @@ __global__ void __launch_bounds__(Launch<S>::BLOCK) k_stft_mag_grad(MagGradArgs 
   const long long f_lo = (s0 >= a.W) ? (s0 - a.W) / a.H + 1 : 0;
   long long f_hi = (s1 - 1) / a.H;
   if (f_hi > a.frames - 1) f_hi = a.frames - 1;
-  const float* pcm = a.pcm + sig * a.sig_stride;
+  const float* pcm = PH ? nullptr : a.pcm + sig * a.sig_stride;
   const float* gsig = a.grad_mag + sig * a.frames * (long long)(M + 1);
-  const float2* w = tw.pyr + ((1 << LN) - 1) + t;  // e^{-2 pi i k / N}, k = t + i*T
+  const float2* psig = PH ? a.phasor + sig * a.frames * (long long)(M + 1) : nullptr;
   __syncthreads();
 
   for (long long f0 = f_lo; f0 <= f_hi; f0 += G) {  // block-uniform loop
     const long long f = f0 + g;
-    const bool ok = f <= f_hi;
     float2 v[R];
-    long long cnt;
-    grad_load<S>(a, pcm, f, ok, t, v, &cnt);
-    fft_engine<S>(v, t, sm, tw);
-
-    // Untangle Z (the M-point transform of z) into X[k], k = t + i*T, and
-    // apply the magnitude chain rule bin by bin.
+    frame_grad_any<S, PH>(a, pcm, psig, gsig, f, f <= f_hi, t, sm, tw, v);
     tile_write_natural<S>(v, t, sm);
-    __syncthreads();
-    const float* gf = gsig + (ok ? f : 0) * (long long)(M + 1);
-    float2 y[R];
-#pragma unroll
-    for (int i = 0; i < R; ++i) {
-      const int k = t + i * T;
-      const float2 zk = v[i];
-      const float2 zm = sm[pidx((M - k) & (M - 1))];
-      const float2 E = make_float2(0.5f * (zk.x + zm.x), 0.5f * (zk.y - zm.y));
-      const float2 D = make_float2(zk.x - zm.x, zk.y + zm.y);
-      const float2 O = make_float2(0.5f * D.y, -0.5f * D.x);
-      float2 X = cadd(E, cmul(__ldg(w + i * T), O));
-      const float gk = ok ? __ldg(gf + k) : 0.f;
-      if (i == 0 && t == 0) {
-        X.y = 0.f;  // DC is real
-        const float2 V = mag_chain(X, gk);
-        y[i] = make_float2(2.f * V.x, 0.f);
-      } else {
-        y[i] = mag_chain(X, gk);
-      }
-    }
-    float2 ynyq = make_float2(0.f, 0.f);
-    if (t == 0) {  // Nyquist X[M] = Re Z[0] - Im Z[0]
-      const float xn = v[0].x - v[0].y;
-      const float gn = ok ? __ldg(gf + M) : 0.f;
-      ynyq = make_float2(2.f * mag_chain(make_float2(xn, 0.f), gn).x, 0.f);
-    }
-    __syncthreads();  // every read of Z is done
-    tile_write_natural<S>(y, t, sm);
-    if (t == 0) sm[pidx(M)] = ynyq;
-    __syncthreads();
-
-    // Hermitian half spectrum Y -> z' with x[2m] = Re, x[2m+1] = Im of the
-    // unnormalised inverse: E = (Y[m] + conj Y[M-m]) / 2,
-    // O = (Y[m] - conj Y[M-m]) e^{+2 pi i m/N} / 2, z' = IDFT_M(E + i O),
-    // the IDFT taken as conj . DFT . conj.
-#pragma unroll
-    for (int i = 0; i < R; ++i) {
-      const int m = t + i * T;
-      const float2 ym = sm[pidx(M - m)];
-      const float2 E = make_float2(0.5f * (y[i].x + ym.x), 0.5f * (y[i].y - ym.y));
-      const float2 D = make_float2(0.5f * (y[i].x - ym.x), 0.5f * (y[i].y + ym.y));
-      const float2 O = cmul(D, cconj(__ldg(w + i * T)));
-      v[i] = make_float2(E.x - O.y, -(E.y + O.x));
-    }
-    __syncthreads();  // the engine reuses the tile
-    fft_engine<S>(v, t, sm, tw);
-
-    // This frame's windowed gradient into its tile: dL/ds[2m] = Re, dL/ds[2m+1] = -Im.
-#pragma unroll
-    for (int i = 0; i < R; ++i) {
-      const int m = t + i * T;
-      const int n = 2 * m;
-      float d0 = v[i].x, d1 = -v[i].y;
-      if (a.win) {
-        d0 *= __ldg(a.win + n);
-        d1 *= __ldg(a.win + n + 1);
-      }
-      if (n >= cnt) d0 = 0.f;
-      if (n + 1 >= cnt) d1 = 0.f;
-      sm[pidx(m)] = make_float2(d0, d1);
-    }
-    __syncthreads();
+    __syncthreads();  // every group's frame is in its tile
 
     // Overlap-add adjoint: each owned sample gathers this round's frames in
     // frame order.
@@ -222,16 +302,120 @@ __global__ void __launch_bounds__(Launch<S>::BLOCK) k_stft_mag_grad(MagGradArgs 
       }
       acc[p - s0] = sum;
     }
-    __syncthreads();
+    __syncthreads();  // tiles are reused by the next round
   }
 
   float* out = a.grad_pcm + sig * a.sig_stride + s0;
   for (int p = threadIdx.x; p < ns; p += B) out[p] = acc[p];
 }
 
+// Sliding form, for hops H = N / 2^QL with H a multiple of 2T: thread t
+// holds samples 2(t + i*T) + {0, 1} of every frame, so the overlap-add
+// partners of a sample in consecutive frames sit in the same thread,
+// SH = H / 2T register slots apart.  Each group of T threads walks a run of
+// `run` consecutive frames of one signal (plus the frames before it that
+// reach into it), adds every frame's gradient into a register window, and
+// after each frame writes the SH slots no later frame touches.  Groups are
+// independent: no block barrier, no accumulator in shared memory.  The
+// sums are taken in frame order, as in the general form.
+// The sliding form also keeps the register window: 3 blocks of 256 threads
+// (85 registers) at radix 8, 2 (128 registers) at radix 16.
+template <class S>
+constexpr int slide_min_blocks() {
+  constexpr int want = S::R <= 8 ? 3 : 2;
+  constexpr int fit80 = 65536 / (Launch<S>::BLOCK * 80);  // blocks at 80 registers a thread
+  return want < fit80 ? want : (fit80 > 1 ? fit80 : 1);
+}
+
+template <class S, int QL, bool PH>
+__global__ void __launch_bounds__(Launch<S>::BLOCK, slide_min_blocks<S>()) k_stft_mag_grad_slide(MagGradArgs a,
+                                                                                                 Twiddles tw) {
+  extern __shared__ float2 smem[];
+  constexpr int T = S::T, R = S::R, M = S::M, G = Launch<S>::G;
+  constexpr int SH = R >> QL;  // register slots per hop
+  static_assert(SH >= 1, "hop of at least 2T samples");
+  const int g = threadIdx.x / T;
+  const int t = threadIdx.x - g * T;
+  float2* sm = smem + g * S::SMEM;
+  const long long runs = (a.frames + a.run - 1) / a.run;
+  const long long job = (long long)blockIdx.x * G + g;
+  if (job >= a.signals * runs) return;  // the whole group leaves; no block barrier follows
+  const long long sig = job / runs;
+  const long long f_own = (job - sig * runs) * a.run;
+  const long long f_end = (f_own + a.run < a.frames) ? f_own + a.run : a.frames;
+  const long long halo = (long long)(1 << QL) - 1;  // earlier frames reaching into f_own*H
+  const long long f_start = (f_own > halo) ? f_own - halo : 0;
+  const float* pcm = PH ? nullptr : a.pcm + sig * a.sig_stride;
+  const float* gsig = a.grad_mag + sig * a.frames * (long long)(M + 1);
+  const float2* psig = PH ? a.phasor + sig * a.frames * (long long)(M + 1) : nullptr;
+  float* out = a.grad_pcm + sig * a.sig_stride;
+  const long long L = a.pcm_len;
+
+  float2 acc[R];
+#pragma unroll
+  for (int i = 0; i < R; ++i) acc[i] = make_float2(0.f, 0.f);
+  for (long long f = f_start; f < f_end; ++f) {
+    float2 v[R];
+    frame_grad_any<S, PH>(a, pcm, psig, gsig, f, true, t, sm, tw, v);
+#pragma unroll
+    for (int i = 0; i < R; ++i) acc[i] = cadd(acc[i], v[i]);
+    if (f >= f_own) {  // samples f*H .. f*H + H - 1 are complete
+      const long long base = f * (long long)a.H;
+#pragma unroll
+      for (int i = 0; i < SH; ++i) {
+        const long long p = base + 2 * (t + i * T);
+        if (p < L) out[p] = acc[i].x;
+        if (p + 1 < L) out[p + 1] = acc[i].y;
+      }
+    }
+#pragma unroll
+    for (int i = 0; i < R; ++i) acc[i] = (i + SH < R) ? acc[i + SH] : make_float2(0.f, 0.f);
+  }
+  if (f_end == a.frames) {
+    // the last run also writes the tail of the last frame and zeros the
+    // samples no frame covers
+    const long long base = f_end * (long long)a.H;
+#pragma unroll
+    for (int i = 0; i < R - SH; ++i) {
+      const long long p = base + 2 * (t + i * T);
+      if (p < L) out[p] = acc[i].x;
+      if (p + 1 < L) out[p + 1] = acc[i].y;
+    }
+    for (long long p = base + 2LL * (R - SH) * T + t; p < L; p += T) out[p] = 0.f;
+  }
+}
+
 }  // namespace
 
 int max_mag_grad_log() { return 14; }
+
+// Radix of the sliding form: FFTFREE_GRAD_LOGR overrides it (sweeps).
+static int slide_logr(int logm) {
+  static const int env = [] {
+    const char* e = std::getenv("FFTFREE_GRAD_LOGR");
+    return e ? std::atoi(e) : 0;
+  }();
+  if (env == 3 || env == 4) return env;
+  return (logm == 10) ? 4 : 3;
+}
+
+template <class S, int QL, bool PH>
+static cudaError_t launch_slide(const MagGradArgs& a, cudaStream_t st, uint64_t* launches) {
+  using L = Launch<S>;
+  const size_t smem = (size_t)L::G * S::SMEM * sizeof(float2);
+  if (smem > 48 * 1024) {
+    const cudaError_t e = cudaFuncSetAttribute(k_stft_mag_grad_slide<S, QL, PH>,
+                                               cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+  }
+  const long long jobs = a.signals * ((a.frames + a.run - 1) / a.run);
+  const long long grid = (jobs + L::G - 1) / L::G;
+  if (grid > 0x7fffffffLL) return cudaErrorInvalidValue;
+  Twiddles tw{twiddle_pyramid(0, st), twiddle_pass_tables(st)};
+  k_stft_mag_grad_slide<S, QL, PH><<<(unsigned)grid, L::BLOCK, smem, st>>>(a, tw);
+  if (launches) ++*launches;
+  return cudaGetLastError();
+}
 
 cudaError_t launch_stft_mag_grad(const MagGradArgs& a, int req_logr, cudaStream_t st, uint64_t* launches) {
   if (a.N < 2 || (a.N & (a.N - 1)) || a.signals <= 0 || a.pcm_len <= 0 || a.frames <= 0 || a.span <= 0 ||
@@ -239,6 +423,37 @@ cudaError_t launch_stft_mag_grad(const MagGradArgs& a, int req_logr, cudaStream_
     return cudaErrorInvalidValue;
   const int logm = ilog2i(a.N) - 1;
   if (logm + 1 > max_mag_grad_log()) return cudaErrorInvalidValue;
+
+  // Sliding form when the hop is N / 2^q (q <= 3) and a multiple of 2T.
+  if (a.run > 0 && logm >= 6 && (a.N % a.H) == 0) {
+    const int q = ilog2i(a.N / a.H);
+    const int lr = slide_logr(logm);
+    const int T = 1 << (logm - lr);
+    if ((1 << q) == a.N / a.H && q <= 3 && (a.H % (2 * T)) == 0) {
+      return with_sched(logm, lr, [&](auto tag) -> cudaError_t {
+        using S = typename decltype(tag)::type;
+        if constexpr (S::LOGM < 6 || (S::LOGR != 3 && S::LOGR != 4) || S::T > 1024) {
+          return cudaErrorInvalidValue;
+        } else {
+          if (a.phasor) {
+            switch (q) {
+              case 0: return launch_slide<S, 0, true>(a, st, launches);
+              case 1: return launch_slide<S, 1, true>(a, st, launches);
+              case 2: return launch_slide<S, 2, true>(a, st, launches);
+              default: return launch_slide<S, 3, true>(a, st, launches);
+            }
+          }
+          switch (q) {
+            case 0: return launch_slide<S, 0, false>(a, st, launches);
+            case 1: return launch_slide<S, 1, false>(a, st, launches);
+            case 2: return launch_slide<S, 2, false>(a, st, launches);
+            default: return launch_slide<S, 3, false>(a, st, launches);
+          }
+        }
+      });
+    }
+  }
+
   const int logr = choose_logr(logm, req_logr, true);
   if (logr < 0) return cudaErrorInvalidValue;
   return with_sched(logm, logr, [&](auto tag) -> cudaError_t {
@@ -249,16 +464,17 @@ cudaError_t launch_stft_mag_grad(const MagGradArgs& a, int req_logr, cudaStream_
       using L = Launch<S>;
       const size_t smem = (size_t)L::G * S::SMEM * sizeof(float2) + (size_t)a.span * sizeof(float);
       if (smem > 227 * 1024) return cudaErrorInvalidValue;
+      const void* fn = a.phasor ? (const void*)k_stft_mag_grad<S, true> : (const void*)k_stft_mag_grad<S, false>;
       if (smem > 48 * 1024) {
-        const cudaError_t e = cudaFuncSetAttribute(k_stft_mag_grad<S>,
-                                                   cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        const cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         if (e != cudaSuccess) return e;
       }
       const long long per_sig = (a.pcm_len + a.span - 1) / a.span;
       const long long grid = per_sig * a.signals;
       if (grid > 0x7fffffffLL) return cudaErrorInvalidValue;
       Twiddles tw{twiddle_pyramid(0, st), twiddle_pass_tables(st)};
-      k_stft_mag_grad<S><<<(unsigned)grid, L::BLOCK, smem, st>>>(a, tw);
+      if (a.phasor) k_stft_mag_grad<S, true><<<(unsigned)grid, L::BLOCK, smem, st>>>(a, tw);
+      else k_stft_mag_grad<S, false><<<(unsigned)grid, L::BLOCK, smem, st>>>(a, tw);
       if (launches) ++*launches;
       return cudaGetLastError();
     }

@@ -37,7 +37,10 @@ struct StftArgs {
   // sig_frames == 0: one signal.
   long long sig_frames;
   long long sig_stride;
-  int mag_only;  // forward R2C half spectrum, only |X| (bins 0..N/2) written
+  // forward R2C half spectrum, bins 0..N/2: 1 = only |X| (out_mag),
+  // 2 = |X| (out_mag) and the unit phasor X / |X| (out_phasor, 0 where |X| = 0)
+  int mag_only;
+  float2* out_phasor;
 };
 
 // Gradient of the magnitude STFT (forward R2C half spectrum, |X| per bin)
@@ -53,8 +56,10 @@ struct MagGradArgs {
   int N, W, H;
   const float* win;       // device, length >= W, or nullptr
   const float* grad_mag;  // (signals * frames) x (N/2 + 1)
+  const float2* phasor;   // saved X / |X|, same layout (0 at |X| = 0); nullptr: recompute from pcm
   float* grad_pcm;        // signals x sig_stride; every sample < pcm_len written
-  int span;               // samples of one signal owned by one block
+  int span;               // general form: samples of one signal owned by one block
+  int run;                // sliding form: frames of one signal per thread group (0: general form only)
 };
 
 // Complex columns in/out with the plan hooks (C++ fft_inplace_batched).

@@ -114,6 +114,22 @@ FFT_CFFI_API size_t fftfree_stft_magnitude(void* handle, const float* pcm, size_
 FFT_CFFI_API size_t fftfree_stft_magnitude_backward(void* handle, const float* pcm, size_t signals,
                                                     size_t length, const float* grad_mag, float* grad_pcm);
 
+/* The forward pass that keeps what the gradient needs instead of the
+ * signal: |X| into out_mag as fftfree_stft_magnitude does, and the unit
+ * phasor X / |X| (0 where |X| = 0) into out_phasor as interleaved
+ * (real, imaginary) float pairs, signals x frames x (N/2 + 1) of them.
+ * Returns the frames per signal, 0 on failure. */
+FFT_CFFI_API size_t fftfree_stft_magnitude_phasor(void* handle, const float* pcm, size_t signals, size_t length,
+                                                  float* out_mag, float* out_phasor, size_t max_frames);
+
+/* fftfree_stft_magnitude_backward from the phasor fftfree_stft_magnitude_phasor
+ * saved instead of the signal: one inverse transform per frame, no forward
+ * transform.  length is the signals' length (it fixes the frames and the last
+ * frame's sample count).  Returns the frames per signal, 0 on failure. */
+FFT_CFFI_API size_t fftfree_stft_magnitude_backward_phasor(void* handle, const float* phasor, size_t signals,
+                                                           size_t length, const float* grad_mag,
+                                                           float* grad_pcm);
+
 /* Test hook of the recovery coordinator (fft_cffi.cpp:954-982): runs the
  * host-side dropout / restore / split decisions for one batch of `frames`
  * frames, invoking the registered restore observer as the recovery path

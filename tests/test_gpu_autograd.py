@@ -62,6 +62,12 @@ CASES = [
     (1, 70000, 16384, 16384, 4096, "hann"),
     (2, 777, 64, 64, 100, "hann"),    # hop > window: samples between frames get 0
     (3, 50, 64, 64, 16, "hann"),      # shorter than the window: one zero-padded frame
+    # sliding-window adjoint (hop N / 2^q, q <= 3): several runs of frames per signal
+    (3, 33333, 512, 400, 256, "hann"),
+    (2, 20000, 128, 128, 16, "hann"),
+    (2, 10000, 256, 256, 256, None),
+    (2, 100, 512, 512, 128, "hann"),
+    (1, 300000, 8192, 8192, 2048, "hann"),
 ]
 
 
@@ -141,20 +147,56 @@ def test_backward_deterministic():
     assert torch.equal(a, b)
 
 
+@pytest.mark.parametrize("S,L,N,W,H,kind", CASES)
+def test_backward_from_saved_phasor(S, L, N, W, H, kind):
+    """The forward pass that saves X / |X| and the backward that starts from it."""
+    x = sinusoids(S, L, 400 + N)
+    g = _loss_grad(x, N, W, H, kind, 500 + N)
+    plan = ag.StftPlan(N, H, W, kind)
+    xt = torch.from_numpy(x).cuda()
+    mag, ph = plan.magnitude_phasor(xt)
+    assert torch.equal(mag, plan.magnitude(xt))  # same kernel, same magnitudes
+    gx = plan.magnitude_backward_phasor(ph, torch.from_numpy(g).cuda(), L).cpu().numpy()
+    ref = grad64.stft_mag_grad64(x, g, N, W, H, window_of(kind, W))
+    err = rel_l2(gx, ref)
+    assert err <= tol(N), err
+    # the saved phasor is X / |X| (checked where |X| is not tiny)
+    F = plan.frames(L)
+    fr = np.zeros((S, F, N))
+    win = window_of(kind, W)
+    for f in range(F):
+        cnt = max(0, min(W, L - f * H))
+        seg = x[:, f * H: f * H + cnt].astype(np.float64)
+        fr[:, f, :cnt] = seg * (win[:cnt] if win is not None else 1.0)
+    X = np.fft.rfft(fr, axis=-1)
+    big = np.abs(X) > 1e-3 * np.abs(X).max()
+    u = ph.cpu().numpy().astype(np.complex128)
+    assert np.max(np.abs(u[big] - X[big] / np.abs(X[big]))) < 1e-3
+    assert np.allclose(np.abs(u[big]), 1.0, atol=1e-6)
+
+
 def test_autograd_function():
+    """Both backward sources through torch.autograd: the saved phase (the
+    default while it fits the plan's budget) and the recomputed spectrum."""
     S, L, N, H = 2, 12000, 512, 128
-    x = torch.from_numpy(sinusoids(S, L, 10)).cuda().requires_grad_(True)
+    x0 = torch.from_numpy(sinusoids(S, L, 10)).cuda()
     T = torch.from_numpy(sinusoids(S, L, 11)).cuda()
-    plan = ag.StftPlan(N, H, N, "hann")
-    tgt = ag.stft_magnitude(T, plan).detach()
-    mag = ag.stft_magnitude(x, plan)
-    loss = (mag - tgt).square().sum()
-    loss.backward()
-    direct = plan.magnitude_backward(x.detach(), 2 * (mag.detach() - tgt))
-    assert torch.equal(x.grad, direct)
-    ref = grad64.stft_mag_grad64(x.detach().cpu().numpy(), (2 * (mag.detach() - tgt)).cpu().numpy(), N, N, H,
-                                 window_of("hann", N))
-    assert rel_l2(x.grad.cpu().numpy(), ref) <= tol(N)
+    for budget, phase_path in ((1 << 30, True), (0, False)):
+        plan = ag.StftPlan(N, H, N, "hann", phase_budget=budget)
+        x = x0.clone().requires_grad_(True)
+        assert plan.stores_phase(x) == phase_path
+        tgt = ag.stft_magnitude(T, plan).detach()
+        mag = ag.stft_magnitude(x, plan)
+        loss = (mag - tgt).square().sum()
+        loss.backward()
+        up = 2 * (mag.detach() - tgt)
+        if phase_path:
+            direct = plan.magnitude_backward_phasor(plan.magnitude_phasor(x.detach())[1], up, L)
+        else:
+            direct = plan.magnitude_backward(x.detach(), up)
+        assert torch.equal(x.grad, direct)
+        ref = grad64.stft_mag_grad64(x.detach().cpu().numpy(), up.cpu().numpy(), N, N, H, window_of("hann", N))
+        assert rel_l2(x.grad.cpu().numpy(), ref) <= tol(N)
 
 
 def test_finite_differences_fp64():
@@ -201,11 +243,12 @@ def test_differentiation_workload_full_size():
     T = plan.magnitude(torch.from_numpy(y).cuda())
     g = 2 * (mag - T)
     gx = plan.magnitude_backward(xt, g).cpu().numpy()
+    gxp = plan.magnitude_backward_phasor(plan.magnitude_phasor(xt)[1], g, L).cpu().numpy()
     mag = mag.cpu().numpy()
     g = g.cpu().numpy()
     assert mag.shape == (S, 509, 1025)
     win = torch.hann_window(N, periodic=False, dtype=torch.float64)
-    num_f = den_f = num_b = den_b = 0.0
+    num_f = den_f = num_b = den_b = num_p = 0.0
     for s0 in range(0, S, 8):
         xs = x[s0: s0 + 8]
         ref = torch.stft(torch.from_numpy(xs.astype(np.float64)), n_fft=N, hop_length=H, window=win, center=False,
@@ -214,13 +257,15 @@ def test_differentiation_workload_full_size():
         den_f += float(np.sum(ref ** 2))
         rb = grad64.stft_mag_grad64(xs, g[s0: s0 + 8], N, N, H, window_of("hann", N))
         num_b += float(np.sum((gx[s0: s0 + 8] - rb) ** 2))
+        num_p += float(np.sum((gxp[s0: s0 + 8] - rb) ** 2))
         den_b += float(np.sum(rb ** 2))
-    ef, eb = math.sqrt(num_f / den_f), math.sqrt(num_b / den_b)
+    ef, eb, ep = math.sqrt(num_f / den_f), math.sqrt(num_b / den_b), math.sqrt(num_p / den_b)
     print(f"differentiation workload: forward rel-L2 {ef:.3e} (vs torch.stft fp64, fp32 taps), "
-          f"backward rel-L2 {eb:.3e}")
+          f"backward rel-L2 {eb:.3e} (recomputed spectrum), {ep:.3e} (saved phasor)")
     # torch's window is the exact float64 Hann, ours the float32 taps: add their rounding
     assert ef <= tol(N) + 1e-6
     assert eb <= tol(N)
+    assert ep <= tol(N)
 
 
 def _griffin_lim_signal(target, N, W, H, L, iters, seed):
