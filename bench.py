@@ -52,10 +52,13 @@ def _peaks():
 def _profile_traffic():
     """DRAM bytes per launch of the C2C kernel from the committed ncu summary."""
     try:
-        with open(os.path.join(REPO, "profiles", "c2c_n4096_traffic.json")) as f:
-            return json.load(f).get("dram_bytes_per_launch")
+        with open(os.path.join(REPO, "profiles", "k_fft_c2c_n4096.md")) as f:
+            for line in f:
+                if line.startswith("traffic_bytes_per_launch:"):
+                    return int(line.split(":", 1)[1])
     except Exception:
-        return None
+        pass
+    return None
 
 
 class ClockSampler:
@@ -159,6 +162,74 @@ def run_reference(args, rank, world):
     return 0
 
 
+# Single-kernel workloads for profiling (ncu -k <kernel> -s <warm-up> -c 1):
+# device-resident inputs larger than L2, one library call per launch.
+CASES = {
+    "c2c_n4096_b8192": "C2C N=4096 x 8192 complex64, Stockham, fftfree_execute_c2c",
+    "stft_n1024_h256": "STFT N=W=1024 H=256 on 128 x 65536 samples, radix option 4, reduce_magnitude, half",
+    "mag_n2048": "magnitude STFT N=W=2048 H=512, 64 x 262144 samples (autograd plain forward)",
+    "mag_phasor_n2048": "magnitude + unit phasor STFT N=W=2048 H=512, 64 x 262144 samples (autograd forward)",
+    "grad_phasor_n2048": "magnitude STFT gradient from the saved phasor, N=W=2048 H=512, 64 x 262144",
+    "grad_recompute_n2048": "magnitude STFT gradient with the spectrum recomputed, N=W=2048 H=512, 64 x 262144",
+}
+
+
+def run_case(args):
+    import torch
+    import fftfree_b200 as ff
+    from fftfree_b200 import autograd as ag
+
+    stream = torch.cuda.Stream()
+    torch.cuda.set_stream(stream)
+    g = torch.Generator(device="cuda").manual_seed(1)
+    name = args.case
+    if name == "c2c_n4096_b8192":
+        x = torch.randn(8192, 4096, 2, device="cuda", generator=g)
+        y = torch.empty_like(x)
+        c = ff.FftContext.full_v2(4096, kernel=2)
+        c.set_stream(stream.cuda_stream)
+        c.set_async(True)
+        fn, nbytes = (lambda: c.execute_c2c(x, y, 8192)), 2 * x.numel() * 4
+    elif name == "stft_n1024_h256":
+        L = 128 * 65536
+        pcm = torch.rand(L, device="cuda", generator=g) * 2 - 1
+        frames, bins = 1 + (L - 1024) // 256, 513
+        re = torch.empty(frames * bins, device="cuda")
+        im, mg = torch.empty_like(re), torch.empty_like(re)
+        c = ff.FftContext.full_v2(1024, kernel=2, radix=4, window=1024, hop=256, transform=1, reduce_magnitude=1,
+                                  half_spectrum=1)
+        c.set_stream(stream.cuda_stream)
+        c.set_async(True)
+        fn, nbytes = (lambda: c.execute_batched(pcm, re, im, mg, pcm_len=L)), L * 4 + 3 * frames * bins * 4
+    else:
+        S, L = 64, 262144
+        x = torch.rand(S, L, device="cuda", generator=g) * 2 - 1
+        plan = ag.StftPlan(2048, 512, 2048, "hann")
+        F, bins = plan.frames(L), plan.bins
+        up = torch.randn(S, F, bins, device="cuda", generator=g)
+        ph = plan.magnitude_phasor(x)[1]
+        spec = S * F * bins * 4
+        fn, nbytes = {
+            "mag_n2048": (lambda: plan.magnitude(x), S * L * 4 + spec),
+            "mag_phasor_n2048": (lambda: plan.magnitude_phasor(x), S * L * 4 + 3 * spec),
+            "grad_phasor_n2048": (lambda: plan.magnitude_backward_phasor(ph, up, L), 3 * spec + S * L * 4),
+            "grad_recompute_n2048": (lambda: plan.magnitude_backward(x, up), 2 * S * L * 4 + spec),
+        }[name]
+    for _ in range(args.warmup):
+        fn()
+    torch.cuda.synchronize()
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a.record(stream)
+    for _ in range(args.steps):
+        fn()
+    b.record(stream)
+    torch.cuda.synchronize()
+    ms = a.elapsed_time(b) / args.steps
+    print(json.dumps({"case": name, "what": CASES[name], "ms": round(ms, 4),
+                      "GB/s": round(nbytes / (ms * 1e-3) / 1e9, 1)}), flush=True)
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -168,12 +239,17 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-legs", action="store_true")
+    ap.add_argument("--case", choices=sorted(CASES),
+                    help="run one kernel workload (W warm-up + K timed launches) and print its timing; "
+                         "the profiling entry point")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.case:
+        return run_case(args)
     if args.impl == "reference":
         return run_reference(args, rank, world)
 

@@ -312,19 +312,79 @@ static size_t frame_count(const FftContext* c, size_t pcm_len, int pad_mode, siz
   return frames;
 }
 
+// ------------------------------------------------------------------ host pipeline
+// A call on host buffers is cut into chunks whose upload (up_stream),
+// kernels (the context stream) and download (down_stream) overlap: chunk
+// i + 1 uploads while chunk i computes and chunk i - 1 downloads, both
+// directions of the host link busy at once.  Pinned host memory lets the
+// copies run asynchronously; pageable memory still works, with less overlap.
+constexpr size_t kPipeChunkBytes = 32u << 20;  // host bytes moved per chunk, about
+constexpr int kPipeMaxChunks = 16;
+
+static int pipe_chunks(size_t host_bytes, long long units) {
+  if (host_bytes < 2 * kPipeChunkBytes || units < 2) return 1;
+  long long n = (long long)(host_bytes / kPipeChunkBytes);
+  n = std::min<long long>(std::min<long long>(n, kPipeMaxChunks), units);
+  return (int)std::max<long long>(n, 1);
+}
+
+static void ensure_pipe(FftContext* c) {
+  if (c->up_stream) return;
+  FFB_CHECK(cudaStreamCreateWithFlags(&c->up_stream, cudaStreamNonBlocking));
+  FFB_CHECK(cudaStreamCreateWithFlags(&c->down_stream, cudaStreamNonBlocking));
+  c->pipe_events.assign(2 * kPipeMaxChunks + 2, nullptr);
+  for (cudaEvent_t& e : c->pipe_events) FFB_CHECK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+}
+
+// Runs `chunks` pieces: up(i, s) enqueues piece i's host->device copies,
+// run(i, s) its kernels, down(i, s) its device->host copies.  On return the
+// context stream is ordered after every copy; the caller synchronises it.
+template <class Up, class Run, class Down>
+static void run_pipelined(FftContext* c, int chunks, Up&& up, Run&& run, Down&& down) {
+  ensure_pipe(c);
+  cudaEvent_t* ev = c->pipe_events.data();
+  cudaEvent_t start = ev[2 * kPipeMaxChunks], done = ev[2 * kPipeMaxChunks + 1];
+  FFB_CHECK(cudaEventRecord(start, c->stream));
+  FFB_CHECK(cudaStreamWaitEvent(c->up_stream, start, 0));
+  FFB_CHECK(cudaStreamWaitEvent(c->down_stream, start, 0));
+  for (int i = 0; i < chunks; ++i) {
+    up(i, c->up_stream);
+    FFB_CHECK(cudaEventRecord(ev[2 * i], c->up_stream));
+    FFB_CHECK(cudaStreamWaitEvent(c->stream, ev[2 * i], 0));
+    run(i, c->stream);
+    FFB_CHECK(cudaEventRecord(ev[2 * i + 1], c->stream));
+    FFB_CHECK(cudaStreamWaitEvent(c->down_stream, ev[2 * i + 1], 0));
+    down(i, c->down_stream);
+  }
+  FFB_CHECK(cudaEventRecord(done, c->down_stream));
+  FFB_CHECK(cudaStreamWaitEvent(c->stream, done, 0));
+}
+
+static void copy_h2d(float* dst, const float* src, size_t count, cudaStream_t s) {
+  if (count) FFB_CHECK(cudaMemcpyAsync(dst, src, count * sizeof(float), cudaMemcpyHostToDevice, s));
+}
+static void copy_d2h(float* dst, const float* src, size_t count, cudaStream_t s) {
+  if (count) FFB_CHECK(cudaMemcpyAsync(dst, src, count * sizeof(float), cudaMemcpyDeviceToHost, s));
+}
+
 // STFT of `frames` frames of `pcm` into (re, im, mag), bins per frame
 // `out_bins`; shared by fft_execute_batched, fft_execute and the one-shot.
 static void run_stft(FftContext* c, const float* pcm, size_t pcm_len, size_t frames, int W, int H,
                      bool use_window, int out_bins, bool mag_from_real, const PostFlags& pf,
                      bool mirror, float* re, float* im, float* mag) {
   const size_t span = std::min(pcm_len, (frames - 1) * (size_t)H + (size_t)W);
-  bool any_host = !is_device_ptr(pcm);
-  const float* d_pcm = stage_in(c, c->d_in0, pcm, span);
+  const bool in_host = !is_device_ptr(pcm);
   const size_t outn = frames * (size_t)out_bins;
   OutTarget o_re = stage_out(c->d_out0, re, outn);
   OutTarget o_im = stage_out(c->d_out1, im, outn);
   OutTarget o_mag = stage_out(c->d_out2, mag, outn);
-  any_host = any_host || o_re.host || o_im.host || o_mag.host;
+  const bool any_host = in_host || o_re.host || o_im.host || o_mag.host;
+  const size_t host_bytes = ((in_host ? span : 0) +
+                             outn * ((o_re.host ? 1 : 0) + (o_im.host ? 1 : 0) + (o_mag.host ? 1 : 0))) * 4;
+  const int chunks = single_pass(c->N, true) ? pipe_chunks(host_bytes, (long long)frames) : 1;
+  // host input is uploaded here, or chunk by chunk by the pipeline below
+  const float* d_pcm = (chunks > 1 && in_host) ? static_cast<const float*>(c->d_in0.get(span * sizeof(float)))
+                                               : stage_in(c, c->d_in0, pcm, span);
   StftArgs a{};
   a.pcm = d_pcm;
   a.pcm_len = (long long)span;
@@ -342,6 +402,50 @@ static void run_stft(FftContext* c, const float* pcm, size_t pcm_len, size_t fra
   a.out_re = o_re.dev;
   a.out_im = o_im.dev;
   a.out_mag = o_mag.dev;
+  if (chunks > 1) {
+    // frames [f0, f1) of chunk i read pcm[f0*H, (f1-1)*H + W); uploads skip
+    // what an earlier chunk already brought over
+    const size_t per = (frames + chunks - 1) / chunks;
+    float* d_in = const_cast<float*>(d_pcm);
+    size_t uploaded = 0;
+    auto range = [&](int i, size_t* f0, size_t* f1) {
+      *f0 = std::min(frames, (size_t)i * per);
+      *f1 = std::min(frames, *f0 + per);
+    };
+    run_pipelined(
+        c, chunks,
+        [&](int i, cudaStream_t s) {
+          size_t f0, f1;
+          range(i, &f0, &f1);
+          if (!in_host || f1 <= f0) return;
+          const size_t hi = std::min(span, (f1 - 1) * (size_t)H + (size_t)W);
+          const size_t lo = std::max(uploaded, f0 * (size_t)H);
+          if (hi > lo) copy_h2d(d_in + lo, pcm + lo, hi - lo, s);
+          uploaded = std::max(uploaded, hi);
+        },
+        [&](int i, cudaStream_t s) {
+          size_t f0, f1;
+          range(i, &f0, &f1);
+          if (f1 <= f0) return;
+          StftArgs b = a;
+          b.pcm = d_pcm + f0 * (size_t)H;
+          b.pcm_len = (long long)(span - f0 * (size_t)H);
+          b.frames = (long long)(f1 - f0);
+          b.out_re = a.out_re + f0 * (size_t)out_bins;
+          b.out_im = a.out_im + f0 * (size_t)out_bins;
+          b.out_mag = a.out_mag + f0 * (size_t)out_bins;
+          FFB_CHECK(launch_stft(b, c->logr_req, s, &c->launches));
+        },
+        [&](int i, cudaStream_t s) {
+          size_t f0, f1;
+          range(i, &f0, &f1);
+          const size_t o = f0 * (size_t)out_bins, n = (f1 - f0) * (size_t)out_bins;
+          for (const OutTarget* t : {&o_re, &o_im, &o_mag})
+            if (t->host) copy_d2h(t->user + o, t->dev + o, n, s);
+        });
+    finish_call(c, true);
+    return;
+  }
   if (single_pass(c->N, true)) {
     FFB_CHECK(launch_stft(a, c->logr_req, c->stream, &c->launches));
   } else {
@@ -653,6 +757,12 @@ FFT_CFFI_API void fft_free(void* handle) {
     c->d_frames.release();
     c->d_meta_tw.release();
     c->d_scratch.release();
+    for (cudaStream_t st : {c->up_stream, c->down_stream})
+      if (st) {
+        cudaStreamSynchronize(st);
+        cudaStreamDestroy(st);
+      }
+    for (cudaEvent_t e : c->pipe_events) cudaEventDestroy(e);
     c->magic = 0;
   }
   delete c;
@@ -894,10 +1004,14 @@ FFT_CFFI_API int fftfree_execute_c2c(void* handle, const float* in, float* out, 
     std::lock_guard<std::recursive_mutex> lk(c->mu);
     DeviceGuard g(c->device);
     const size_t n = batch * (size_t)c->N * 2;
-    bool any_host = !is_device_ptr(in);
-    const float* d_in = stage_in(c, c->d_in0, in, n);
+    const bool in_host = !is_device_ptr(in);
     OutTarget o = stage_out(c->d_out0, out, n);
-    any_host = any_host || o.host;
+    const bool any_host = in_host || o.host;
+    const int chunks = single_pass(c->N, false)
+                           ? pipe_chunks(n * 4 * ((in_host ? 1 : 0) + (o.host ? 1 : 0)), (long long)batch)
+                           : 1;
+    const float* d_in = (chunks > 1 && in_host) ? static_cast<const float*>(c->d_in0.get(n * sizeof(float)))
+                                                : stage_in(c, c->d_in0, in, n);
     C2cArgs a{};
     a.in = reinterpret_cast<const float2*>(d_in);
     a.out = reinterpret_cast<float2*>(o.dev);
@@ -908,6 +1022,37 @@ FFT_CFFI_API int fftfree_execute_c2c(void* handle, const float* in, float* out, 
     a.polar_in = c->store_polar ? 1 : 0;
     a.inverse = c->inverse ? 1 : 0;
     a.pf = c->post_flags();
+    if (chunks > 1) {
+      const size_t per = (batch + chunks - 1) / chunks, row = (size_t)c->N * 2;
+      auto rows = [&](int i, size_t* r0, size_t* r1) {
+        *r0 = std::min(batch, (size_t)i * per);
+        *r1 = std::min(batch, *r0 + per);
+      };
+      run_pipelined(
+          c, chunks,
+          [&](int i, cudaStream_t s) {
+            size_t r0, r1;
+            rows(i, &r0, &r1);
+            if (in_host) copy_h2d(const_cast<float*>(d_in) + r0 * row, in + r0 * row, (r1 - r0) * row, s);
+          },
+          [&](int i, cudaStream_t s) {
+            size_t r0, r1;
+            rows(i, &r0, &r1);
+            if (r1 <= r0) return;
+            C2cArgs b = a;
+            b.in = a.in + r0 * (size_t)c->N;
+            b.out = a.out + r0 * (size_t)c->N;
+            b.batch = (long long)(r1 - r0);
+            FFB_CHECK(launch_c2c(b, c->logr_req, s, &c->launches));
+          },
+          [&](int i, cudaStream_t s) {
+            size_t r0, r1;
+            rows(i, &r0, &r1);
+            if (o.host) copy_d2h(o.user + r0 * row, o.dev + r0 * row, (r1 - r0) * row, s);
+          });
+      finish_call(c, true);
+      return 1;
+    }
     if (single_pass(c->N, false)) {
       FFB_CHECK(launch_c2c(a, c->logr_req, c->stream, &c->launches));
     } else {
