@@ -69,6 +69,21 @@ __device__ __forceinline__ float2 tw_get(const Twiddles& tw, int L, unsigned e) 
   return __ldg(tw.pyr + ((1u << L) - 1u) + (e & ((1u << L) - 1u)));
 }
 
+// exp(-2 pi i e / 2^L) for the inter-pass twiddles of the multi-pass
+// kernels, as the product of two short runs of the pyramid:
+// w_{2^L}^e = w_{2^(L-LH)}^(e >> LH) * w_{2^L}^(e & (2^LH - 1)), LH = ceil(L/2).
+// A warp's exponents n2 * k1 scatter over the whole level-L table; the two
+// factors come from 2^(L-LH) and 2^LH contiguous entries that stay in L1
+// (one extra rounding: the product of two correctly rounded factors).
+__device__ __forceinline__ float2 tw_split(const Twiddles& tw, int L, unsigned e) {
+  const int LH = (L + 1) >> 1;
+  const unsigned mask = (1u << L) - 1u;
+  e &= mask;
+  const float2 hi = __ldg(tw.pyr + ((1u << (L - LH)) - 1u) + (e >> LH));
+  const float2 lo = __ldg(tw.pyr + ((1u << L) - 1u) + (e & ((1u << LH) - 1u)));
+  return cmul(hi, lo);
+}
+
 // exp(-2*pi*i*m/16)
 __device__ __forceinline__ float2 w16(int m) {
   constexpr float c1 = 0.92387953251128675613f;  // cos(pi/8)

@@ -62,7 +62,7 @@ k_four_a(IO io, float2* __restrict__ scratch, long long b0, int LN, Twiddles tw)
 #pragma unroll
   for (int i = 0; i < S1::R; ++i) {
     const int k1 = t + i * T1;
-    out[(long long)k1 * N2 + n2] = cmul(v[i], tw_get(tw, LN, (unsigned)(n2 * k1)));
+    out[(long long)k1 * N2 + n2] = cmul(v[i], tw_split(tw, LN, (unsigned)(n2 * k1)));
   }
 }
 
