@@ -437,7 +437,53 @@ def measure_legs(ff, torch, stream, reps: int = 10):
         frames / (legs["stft_r2c_n1024_h256_long_signal"]["ms"] * 1e-3), 1)
     c.close()
     legs["autograd_stft_magnitude"] = measure_autograd(torch, stream, timed)
+    legs["ragged_r2c_4096"] = measure_ragged(ff, torch, stream, timed)
     return legs
+
+
+def measure_ragged(ff, torch, stream, timed):
+    """Ragged batch: 4096 real signals, N = 2^e with e uniform in 6..16 drawn
+    from seed 2, then each signal uniform[-1, 1) from the same generator; R2C
+    half spectrum, planar re / im / mag outputs.  One persistent launch (a
+    CUDA graph) against one fft_execute_batched call per signal on a context
+    per size, the reference's usage (device buffers, enqueued back to back)."""
+    import numpy as np
+
+    rng = np.random.default_rng(2)
+    e = rng.integers(6, 17, 4096)
+    sizes = [1 << int(v) for v in e]
+    pcm_h = np.concatenate([rng.uniform(-1, 1, n) for n in sizes]).astype(np.float32)
+    plan = ff.RaggedPlan(sizes)
+    plan.set_stream(stream.cuda_stream)
+    pcm = torch.from_numpy(pcm_h).cuda()
+    re, im, mag = (torch.empty(plan.bins, device="cuda") for _ in range(3))
+    nbytes = plan.samples * 4 + 3 * plan.bins * 4
+    one = timed(lambda: plan.execute(pcm, re, im, mag), nbytes)
+    ctxs = {}
+    for n in set(sizes):
+        c = ff.FftContext.full_v2(n, kernel=2, pad_mode=1, window=n, hop=n, transform=1, half_spectrum=1)
+        c.set_stream(stream.cuda_stream)
+        c.set_async(True)
+        ctxs[n] = c
+    offs, po, ob = [], 0, 0
+    for n in sizes:
+        offs.append((n, po, ob))
+        po += n
+        ob += n // 2 + 1
+    base_pcm, base_re, base_im, base_mg = pcm.data_ptr(), re.data_ptr(), im.data_ptr(), mag.data_ptr()
+
+    def per_signal():
+        for n, p0, o0 in offs:
+            ctxs[n].execute_batched(base_pcm + 4 * p0, base_re + 4 * o0, base_im + 4 * o0, base_mg + 4 * o0,
+                                    pcm_len=n)
+
+    sep = timed(per_signal, nbytes)
+    for c in ctxs.values():
+        c.close()
+    plan.close()
+    return {"signals": len(sizes), "samples": int(pcm_h.size), "bytes": nbytes, "one_launch": one,
+            "per_signal_launches": sep, "speedup": round(sep["ms"] / one["ms"], 2),
+            "transforms_per_s": round(len(sizes) / (one["ms"] * 1e-3), 1)}
 
 
 def measure_autograd(torch, stream, timed):

@@ -107,6 +107,15 @@ _SIGS = [
                                                        ctypes.c_size_t, c_float_p, c_float_p, ctypes.c_size_t]),
     ("fftfree_stft_magnitude_backward_phasor", ctypes.c_size_t, [ctypes.c_void_p, c_float_p, ctypes.c_size_t,
                                                                 ctypes.c_size_t, c_float_p, c_float_p]),
+    ("fftfree_ragged_plan", ctypes.c_void_p, [ctypes.POINTER(ctypes.c_size_t), ctypes.c_size_t, ctypes.c_int,
+                                              ctypes.c_int]),
+    ("fftfree_ragged_samples", ctypes.c_size_t, [ctypes.c_void_p]),
+    ("fftfree_ragged_bins", ctypes.c_size_t, [ctypes.c_void_p]),
+    ("fftfree_ragged_schedule", ctypes.c_int, [ctypes.c_void_p, ctypes.c_size_t]),
+    ("fftfree_ragged_set_stream", None, [ctypes.c_void_p, ctypes.c_void_p]),
+    ("fftfree_ragged_execute", ctypes.c_int, [ctypes.c_void_p, c_float_p, c_float_p, c_float_p, c_float_p]),
+    ("fftfree_ragged_launch_count", ctypes.c_ulonglong, [ctypes.c_void_p]),
+    ("fftfree_ragged_free", None, [ctypes.c_void_p]),
     ("fftfree_debug_recovery_plan", ctypes.c_size_t, [ctypes.c_size_t, ctypes.c_char_p]),
 ]
 
@@ -273,6 +282,49 @@ class FftContext:
     def stft_magnitude_backward(self, pcm, signals, length, grad_mag, grad_pcm) -> int:
         return int(lib().fftfree_stft_magnitude_backward(self.handle, _fp(pcm), signals, length, _fp(grad_mag),
                                                          _fp(grad_pcm)))
+
+
+class RaggedPlan:
+    """One persistent launch over real signals of mixed sizes (see
+    fftfree_ragged_plan in include/fftfree_b200.h)."""
+
+    def __init__(self, sizes, reduce_magnitude=0, store_polar=0):
+        self.sizes = [int(n) for n in sizes]
+        arr = (ctypes.c_size_t * len(self.sizes))(*self.sizes)
+        self.handle = lib().fftfree_ragged_plan(arr, len(self.sizes), reduce_magnitude, store_polar)
+        if not self.handle:
+            raise RuntimeError("fftfree_ragged_plan failed")
+
+    @property
+    def samples(self) -> int:
+        return int(lib().fftfree_ragged_samples(self.handle))
+
+    @property
+    def bins(self) -> int:
+        return int(lib().fftfree_ragged_bins(self.handle))
+
+    def schedule(self, n) -> int:
+        return int(lib().fftfree_ragged_schedule(self.handle, n))
+
+    def set_stream(self, stream_handle):
+        lib().fftfree_ragged_set_stream(self.handle, ctypes.c_void_p(stream_handle or 0))
+
+    def execute(self, pcm, out_real, out_imag, out_mag) -> int:
+        return int(lib().fftfree_ragged_execute(self.handle, _fp(pcm), _fp(out_real), _fp(out_imag), _fp(out_mag)))
+
+    def launch_count(self) -> int:
+        return int(lib().fftfree_ragged_launch_count(self.handle))
+
+    def close(self):
+        if self.handle:
+            lib().fftfree_ragged_free(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 def device_available() -> bool:

@@ -121,6 +121,30 @@ cudaError_t launch_ola(const OlaArgs& a, cudaStream_t s, uint64_t* launches);
 int max_mag_grad_log();
 cudaError_t launch_stft_mag_grad(const MagGradArgs& a, int logr, cudaStream_t s, uint64_t* launches);
 
+// Ragged batch: one persistent launch over items of different sizes (R2C,
+// half spectrum, one full frame per item).  tiles[i] = {first item, items,
+// log2 complex points, pass radix (log2; 0 for the three-phase sizes)};
+// items are listed in tile order, with their signal and output offsets.
+struct RaggedArgs {
+  const float* pcm;
+  float* out_re;
+  float* out_im;
+  float* out_mag;
+  const long long* pcm_off;
+  const long long* out_off;
+  const int4* tiles;
+  int ntiles;
+  int* counter;     // tiles handed out; zero before each launch
+  float2* scratch;  // ragged_scratch_per_block() bytes per block
+  PostFlags pf;
+};
+int ragged_max_log();                 // largest log2 N
+bool ragged_large_log(int logm);      // sizes that take the three-phase path
+size_t ragged_scratch_per_block();
+int ragged_candidates(int logm, int* lrs);  // pass radices (log2) a size may use; 0 for three-phase
+int ragged_grid();                    // persistent blocks for the current device
+cudaError_t launch_ragged(const RaggedArgs& a, int grid, cudaStream_t s, uint64_t* launches);
+
 // Multi-pass (four-step) transforms for 2^14 <= N <= 2^20.  `scratch` holds
 // `chunk` transforms of N complex points (four_step_chunk picks a chunk
 // that stays resident in L2).

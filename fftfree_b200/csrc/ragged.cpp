@@ -1,0 +1,421 @@
+// ragged.cpp -- ragged batches of real transforms of mixed sizes in one
+// persistent launch: the work list, the per-size schedule autotuner and its
+// on-disk cache, the CUDA graph of the launch, and the C ABI
+// (fftfree_ragged_*).
+//
+// The reference has no ragged entry point: its callers create one context
+// per transform size and loop over the transforms (fft_init_full +
+// fft_execute_batched per size).  An item here gives the same outputs as
+// fft_execute_batched on a context (n_i, window = hop = n_i, transform = R2C,
+// half_spectrum = 1, reduce_magnitude / store_polar as the plan's flags)
+// for one frame of n_i samples.
+#include <cuda_runtime.h>
+#include <sys/stat.h>
+
+#include <algorithm>
+#include <cstdio>
+#include <cstdlib>
+#include <fstream>
+#include <map>
+#include <mutex>
+#include <sstream>
+#include <string>
+#include <tuple>
+#include <vector>
+
+#include "../../include/fftfree_b200.h"
+#include "context.h"
+#include "kernels.h"
+
+namespace ffb {
+namespace {
+
+constexpr uint32_t kRaggedMagic = 0x52414744u;  // "RAGD"
+
+struct RaggedPlan {
+  uint32_t magic = kRaggedMagic;
+  int device = 0;
+  cudaStream_t own_stream = nullptr;
+  cudaStream_t stream = nullptr;
+  std::vector<int> logm;               // per item (caller order): log2 of N/2
+  std::vector<long long> in_off, out_off;  // per item (caller order)
+  size_t samples = 0, bins = 0;
+  PostFlags pf{};
+  int lr[16] = {};                     // pass radix (log2) per log2 N/2 of the single-pass sizes
+  int grid = 0, ntiles = 0;
+  DevBuf d_pcm_off, d_out_off, d_tiles, d_counter, d_scratch, d_in, d_re, d_im, d_mag;
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  const void* graph_ptrs[4] = {};
+  uint64_t launches = 0;
+  std::mutex mu;
+};
+
+RaggedPlan* as_plan(void* h) {
+  auto* p = static_cast<RaggedPlan*>(h);
+  return (p && p->magic == kRaggedMagic) ? p : nullptr;
+}
+
+#define RG_CHECK(expr)                                                                 \
+  do {                                                                                 \
+    cudaError_t _e = (expr);                                                           \
+    if (_e != cudaSuccess) {                                                           \
+      std::fprintf(stderr, "[fftfree_b200] ragged: CUDA error %s at %s:%d\n",          \
+                   cudaGetErrorName(_e), __FILE__, __LINE__);                          \
+      throw std::runtime_error("cuda");                                                \
+    }                                                                                  \
+  } while (0)
+
+int log2_exact(size_t v) {
+  if (v == 0 || (v & (v - 1))) return -1;
+  int l = 0;
+  while ((size_t(1) << l) < v) ++l;
+  return l;
+}
+
+bool is_device(const void* p) {
+  cudaPointerAttributes at;
+  if (!p || cudaPointerGetAttributes(&at, p) != cudaSuccess) {
+    cudaGetLastError();
+    return false;
+  }
+  return at.type == cudaMemoryTypeDevice || at.type == cudaMemoryTypeManaged;
+}
+
+// ---------------------------------------------------------------- work list
+// Tiles of same-size items in work order (largest sizes first); `only` >= 0
+// restricts the list to one size (the tuner).
+struct WorkList {
+  std::vector<int4> tiles;
+  std::vector<long long> pcm_off, out_off;
+};
+
+WorkList build_work(const RaggedPlan& p, int only) {
+  WorkList w;
+  std::vector<std::vector<int>> by(ragged_max_log());
+  for (size_t i = 0; i < p.logm.size(); ++i) by[p.logm[i]].push_back((int)i);
+  for (int L = ragged_max_log() - 1; L >= 0; --L) {
+    if (by[L].empty() || (only >= 0 && L != only)) continue;
+    const bool large = ragged_large_log(L);
+    const int per = large ? 1 : std::max(1, 256 / std::max(1, (1 << L) >> p.lr[L]));
+    for (size_t s = 0; s < by[L].size(); s += per) {
+      const int n = (int)std::min<size_t>(per, by[L].size() - s);
+      w.tiles.push_back(make_int4((int)w.pcm_off.size(), n, L, large ? 0 : p.lr[L]));
+      for (int k = 0; k < n; ++k) {
+        const int i = by[L][s + k];
+        w.pcm_off.push_back(p.in_off[i]);
+        w.out_off.push_back(p.out_off[i]);
+      }
+    }
+  }
+  return w;
+}
+
+void upload(RaggedPlan& p, const WorkList& w) {
+  RG_CHECK(cudaMemcpyAsync(p.d_pcm_off.get(w.pcm_off.size() * 8), w.pcm_off.data(), w.pcm_off.size() * 8,
+                           cudaMemcpyHostToDevice, p.stream));
+  RG_CHECK(cudaMemcpyAsync(p.d_out_off.get(w.out_off.size() * 8), w.out_off.data(), w.out_off.size() * 8,
+                           cudaMemcpyHostToDevice, p.stream));
+  RG_CHECK(cudaMemcpyAsync(p.d_tiles.get(w.tiles.size() * sizeof(int4)), w.tiles.data(),
+                           w.tiles.size() * sizeof(int4), cudaMemcpyHostToDevice, p.stream));
+  RG_CHECK(cudaStreamSynchronize(p.stream));
+  p.ntiles = (int)w.tiles.size();
+}
+
+RaggedArgs args_for(RaggedPlan& p, const float* pcm, float* re, float* im, float* mag) {
+  RaggedArgs a{};
+  a.pcm = pcm;
+  a.out_re = re;
+  a.out_im = im;
+  a.out_mag = mag;
+  a.pcm_off = static_cast<const long long*>(p.d_pcm_off.p);
+  a.out_off = static_cast<const long long*>(p.d_out_off.p);
+  a.tiles = static_cast<const int4*>(p.d_tiles.p);
+  a.ntiles = p.ntiles;
+  a.counter = static_cast<int*>(p.d_counter.p);
+  a.scratch = static_cast<float2*>(p.d_scratch.p);
+  a.pf = p.pf;
+  return a;
+}
+
+// ---------------------------------------------------------------- autotuner
+// Cache of measured choices, keyed by (N, items of that N, transform):
+// FFTFREE_TUNE_CACHE names the file (default ~/.cache/fftfree_b200/tune.txt);
+// FFTFREE_TUNE=0 turns tuning off (the default schedule of the size).
+std::mutex g_cache_mu;
+std::map<std::tuple<long long, long long, std::string>, int> g_cache;
+bool g_cache_loaded = false;
+
+std::string cache_path() {
+  if (const char* e = std::getenv("FFTFREE_TUNE_CACHE")) return e;
+  const char* home = std::getenv("HOME");
+  return std::string(home ? home : ".") + "/.cache/fftfree_b200/tune.txt";
+}
+
+void cache_load() {
+  if (g_cache_loaded) return;
+  g_cache_loaded = true;
+  std::ifstream f(cache_path());
+  std::string line;
+  while (std::getline(f, line)) {
+    std::istringstream s(line);
+    std::string kind, tr;
+    long long n = 0, batch = 0;
+    int lr = 0;
+    if (s >> kind >> tr >> n >> batch >> lr && kind == "ragged" && lr >= 2 && lr <= 5)
+      g_cache[{n, batch, tr}] = lr;
+  }
+}
+
+void cache_store(long long n, long long batch, const std::string& tr, int lr) {
+  g_cache[{n, batch, tr}] = lr;
+  const std::string path = cache_path();
+  const size_t slash = path.find_last_of('/');
+  if (slash != std::string::npos) {
+    // create the cache folder, one level at a time
+    const std::string dir = path.substr(0, slash);
+    for (size_t i = 1; i <= dir.size(); ++i)
+      if (i == dir.size() || dir[i] == '/') (void)mkdir(dir.substr(0, i).c_str(), 0755);
+  }
+  std::ofstream f(path, std::ios::app);
+  if (f) f << "ragged " << tr << " " << n << " " << batch << " " << lr << "\n";
+}
+
+bool tuning_on() {
+  const char* e = std::getenv("FFTFREE_TUNE");
+  return !(e && e[0] == '0');
+}
+
+float time_launch(RaggedPlan& p, const RaggedArgs& a) {
+  cudaEvent_t e0, e1;
+  RG_CHECK(cudaEventCreate(&e0));
+  RG_CHECK(cudaEventCreate(&e1));
+  float best = 1e30f;
+  for (int rep = 0; rep < 4; ++rep) {
+    RG_CHECK(cudaMemsetAsync(a.counter, 0, sizeof(int), p.stream));
+    RG_CHECK(cudaEventRecord(e0, p.stream));
+    RG_CHECK(launch_ragged(a, p.grid, p.stream, &p.launches));
+    RG_CHECK(cudaEventRecord(e1, p.stream));
+    RG_CHECK(cudaEventSynchronize(e1));
+    float ms = 0.f;
+    RG_CHECK(cudaEventElapsedTime(&ms, e0, e1));
+    if (rep > 0) best = std::min(best, ms);  // the first one warms up
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  return best;
+}
+
+void tune(RaggedPlan& p) {
+  std::vector<long long> count(ragged_max_log(), 0);
+  for (int L : p.logm) ++count[L];
+  std::lock_guard<std::mutex> lk(g_cache_mu);
+  cache_load();
+  for (int L = 0; L < ragged_max_log(); ++L) {
+    int cand[4];
+    const int nc = ragged_candidates(L, cand);
+    if (!count[L] || nc == 0) continue;
+    // default: the single-pass kernels' choice for real input, within the candidates
+    int def = choose_logr(L, -1, true);
+    if (std::find(cand, cand + nc, def) == cand + nc) def = cand[nc - 1];
+    p.lr[L] = def;
+    if (nc == 1 || !tuning_on()) continue;
+    const long long n = 2LL << L;
+    auto it = g_cache.find({n, count[L], "r2c"});
+    if (it != g_cache.end() && std::find(cand, cand + nc, it->second) != cand + nc) {
+      p.lr[L] = it->second;
+      continue;
+    }
+    float best = 1e30f;
+    int pick = def;
+    for (int c = 0; c < nc; ++c) {
+      p.lr[L] = cand[c];
+      upload(p, build_work(p, L));
+      const RaggedArgs a = args_for(p, static_cast<const float*>(p.d_in.p), static_cast<float*>(p.d_re.p),
+                                    static_cast<float*>(p.d_im.p), static_cast<float*>(p.d_mag.p));
+      const float ms = time_launch(p, a);
+      if (ms < best) {
+        best = ms;
+        pick = cand[c];
+      }
+    }
+    p.lr[L] = pick;
+    cache_store(n, count[L], "r2c", pick);
+  }
+}
+
+// ---------------------------------------------------------------- graph
+void capture(RaggedPlan& p, const float* pcm, float* re, float* im, float* mag) {
+  const void* key[4] = {pcm, re, im, mag};
+  if (p.exec && std::equal(key, key + 4, p.graph_ptrs)) return;
+  if (p.exec) {
+    cudaGraphExecDestroy(p.exec);
+    cudaGraphDestroy(p.graph);
+    p.exec = nullptr;
+    p.graph = nullptr;
+  }
+  const RaggedArgs a = args_for(p, pcm, re, im, mag);
+  RG_CHECK(cudaStreamBeginCapture(p.stream, cudaStreamCaptureModeThreadLocal));
+  cudaError_t e1 = cudaMemsetAsync(a.counter, 0, sizeof(int), p.stream);
+  cudaError_t e2 = (e1 == cudaSuccess) ? launch_ragged(a, p.grid, p.stream, nullptr) : e1;
+  cudaGraph_t g = nullptr;
+  const cudaError_t e3 = cudaStreamEndCapture(p.stream, &g);
+  RG_CHECK(e1);
+  RG_CHECK(e2);
+  RG_CHECK(e3);
+  p.graph = g;
+  RG_CHECK(cudaGraphInstantiate(&p.exec, g, 0));
+  std::copy(key, key + 4, p.graph_ptrs);
+}
+
+struct Guard {
+  int prev = -1;
+  explicit Guard(int dev) {
+    cudaGetDevice(&prev);
+    if (prev != dev) cudaSetDevice(dev);
+  }
+  ~Guard() {
+    int cur = -1;
+    cudaGetDevice(&cur);
+    if (prev >= 0 && cur != prev) cudaSetDevice(prev);
+  }
+};
+
+}  // namespace
+}  // namespace ffb
+
+using namespace ffb;
+
+extern "C" {
+
+FFT_CFFI_API void* fftfree_ragged_plan(const size_t* sizes, size_t count, int reduce_magnitude,
+                                       int store_polar) {
+  if (!sizes || count == 0 || count > (size_t)1 << 30) return nullptr;
+  RaggedPlan* p = nullptr;
+  try {
+    p = new RaggedPlan();
+    RG_CHECK(cudaGetDevice(&p->device));
+    p->logm.resize(count);
+    p->in_off.resize(count);
+    p->out_off.resize(count);
+    for (size_t i = 0; i < count; ++i) {
+      const int lg = log2_exact(sizes[i]);
+      if (lg < 2 || lg > ragged_max_log()) {
+        std::fprintf(stderr, "[fftfree_b200] fftfree_ragged_plan: size %zu of item %zu is not a power of two "
+                             "in [4, %d]\n", sizes[i], i, 1 << ragged_max_log());
+        delete p;
+        return nullptr;
+      }
+      p->logm[i] = lg - 1;
+      p->in_off[i] = (long long)p->samples;
+      p->out_off[i] = (long long)p->bins;
+      p->samples += sizes[i];
+      p->bins += sizes[i] / 2 + 1;
+    }
+    p->pf.r2c_half = 1;
+    p->pf.polar = store_polar ? 1 : 0;
+    p->pf.reduce = (!store_polar && reduce_magnitude) ? 1 : 0;
+    RG_CHECK(cudaStreamCreateWithFlags(&p->own_stream, cudaStreamNonBlocking));
+    p->stream = p->own_stream;
+    (void)twiddle_pyramid(ragged_max_log(), p->stream);  // built before any capture
+    if (!twiddle_pass_tables(p->stream)) throw std::runtime_error("twiddle tables");
+    p->grid = ragged_grid();
+    p->d_counter.get(sizeof(int));
+    bool any_large = false;
+    for (int L : p->logm) any_large = any_large || ragged_large_log(L);
+    if (any_large) p->d_scratch.get((size_t)p->grid * ragged_scratch_per_block());
+    // staging (host buffers) and the tuner's buffers
+    RG_CHECK(cudaMemsetAsync(p->d_in.get(p->samples * 4), 0, p->samples * 4, p->stream));
+    p->d_re.get(p->bins * 4);
+    p->d_im.get(p->bins * 4);
+    p->d_mag.get(p->bins * 4);
+    tune(*p);
+    upload(*p, build_work(*p, -1));
+    return p;
+  } catch (...) {
+    delete p;
+    return nullptr;
+  }
+}
+
+FFT_CFFI_API size_t fftfree_ragged_samples(void* plan) {
+  RaggedPlan* p = as_plan(plan);
+  return p ? p->samples : 0;
+}
+
+FFT_CFFI_API size_t fftfree_ragged_bins(void* plan) {
+  RaggedPlan* p = as_plan(plan);
+  return p ? p->bins : 0;
+}
+
+FFT_CFFI_API int fftfree_ragged_schedule(void* plan, size_t n) {
+  RaggedPlan* p = as_plan(plan);
+  const int lg = log2_exact(n);
+  if (!p || lg < 2 || lg > ragged_max_log()) return 0;
+  return ragged_large_log(lg - 1) ? 0 : (1 << p->lr[lg - 1]);
+}
+
+FFT_CFFI_API void fftfree_ragged_set_stream(void* plan, void* stream) {
+  RaggedPlan* p = as_plan(plan);
+  if (!p) return;
+  std::lock_guard<std::mutex> lk(p->mu);
+  p->stream = stream ? static_cast<cudaStream_t>(stream) : p->own_stream;
+}
+
+FFT_CFFI_API int fftfree_ragged_execute(void* plan, const float* pcm, float* out_real, float* out_imag,
+                                        float* out_mag) {
+  RaggedPlan* p = as_plan(plan);
+  if (!p || !pcm || !out_real || !out_imag || !out_mag) return 0;
+  try {
+    std::lock_guard<std::mutex> lk(p->mu);
+    Guard g(p->device);
+    const bool in_host = !is_device(pcm);
+    float* outs[3] = {out_real, out_imag, out_mag};
+    DevBuf* stage[3] = {&p->d_re, &p->d_im, &p->d_mag};
+    float* dev_out[3];
+    bool out_host[3];
+    for (int k = 0; k < 3; ++k) {
+      out_host[k] = !is_device(outs[k]);
+      dev_out[k] = out_host[k] ? static_cast<float*>(stage[k]->p) : outs[k];
+    }
+    const float* d_pcm = pcm;
+    if (in_host) {
+      RG_CHECK(cudaMemcpyAsync(p->d_in.p, pcm, p->samples * 4, cudaMemcpyHostToDevice, p->stream));
+      d_pcm = static_cast<const float*>(p->d_in.p);
+    }
+    capture(*p, d_pcm, dev_out[0], dev_out[1], dev_out[2]);
+    RG_CHECK(cudaGraphLaunch(p->exec, p->stream));
+    ++p->launches;
+    bool any_host = in_host;
+    for (int k = 0; k < 3; ++k)
+      if (out_host[k]) {
+        RG_CHECK(cudaMemcpyAsync(outs[k], dev_out[k], p->bins * 4, cudaMemcpyDeviceToHost, p->stream));
+        any_host = true;
+      }
+    if (any_host) RG_CHECK(cudaStreamSynchronize(p->stream));
+    return 1;
+  } catch (...) {
+    return 0;
+  }
+}
+
+FFT_CFFI_API unsigned long long fftfree_ragged_launch_count(void* plan) {
+  RaggedPlan* p = as_plan(plan);
+  return p ? p->launches : 0;
+}
+
+FFT_CFFI_API void fftfree_ragged_free(void* plan) {
+  RaggedPlan* p = as_plan(plan);
+  if (!p) return;
+  {
+    Guard g(p->device);
+    cudaStreamSynchronize(p->stream);
+    if (p->exec) cudaGraphExecDestroy(p->exec);
+    if (p->graph) cudaGraphDestroy(p->graph);
+    if (p->own_stream) cudaStreamDestroy(p->own_stream);
+    p->magic = 0;
+  }
+  delete p;
+}
+
+}  // extern "C"

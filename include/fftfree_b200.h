@@ -130,6 +130,40 @@ FFT_CFFI_API size_t fftfree_stft_magnitude_backward_phasor(void* handle, const f
                                                            size_t length, const float* grad_mag,
                                                            float* grad_pcm);
 
+/* Ragged batches.  No counterpart in the reference, whose callers create
+ * one context per transform size and loop over the transforms
+ * (fft_init_full + fft_execute_batched per size).  A plan covers `count`
+ * real signals of sizes[i] samples each (powers of two, 4 .. 65536), packed
+ * back to back; item i gives what fft_execute_batched gives for one frame of
+ * it on a context (sizes[i], window = hop = sizes[i], transform = R2C,
+ * half_spectrum = 1, the plan's reduce_magnitude / store_polar): planar
+ * re / im / mag rows of sizes[i]/2 + 1 bins, packed back to back in item
+ * order.  All items run in one persistent kernel launch (captured once in a
+ * CUDA graph per set of buffers); the pass radix of each size is chosen by
+ * timing the candidates on the plan's own items at plan time, cached in
+ * FFTFREE_TUNE_CACHE (default ~/.cache/fftfree_b200/tune.txt) keyed by
+ * (size, items of that size, transform); FFTFREE_TUNE=0 keeps the defaults.
+ * The plan lives on the device current at creation.  Returns NULL on a bad
+ * size or a CUDA failure. */
+FFT_CFFI_API void* fftfree_ragged_plan(const size_t* sizes, size_t count, int reduce_magnitude,
+                                       int store_polar);
+/* Total input samples / output bins per array of a plan (0 for NULL). */
+FFT_CFFI_API size_t fftfree_ragged_samples(void* plan);
+FFT_CFFI_API size_t fftfree_ragged_bins(void* plan);
+/* The pass radix the plan runs for size n (0: n is absent from the plan's
+ * single-pass sizes, or takes the three-phase path). */
+FFT_CFFI_API int fftfree_ragged_schedule(void* plan, size_t n);
+/* Stream of the plan's launches (NULL: the plan's own stream). */
+FFT_CFFI_API void fftfree_ragged_set_stream(void* plan, void* cuda_stream);
+/* Runs the plan: host or device buffers (host ones are staged and the call
+ * waits; with device buffers it returns once the launch is enqueued).
+ * Returns 1, or 0 on failure. */
+FFT_CFFI_API int fftfree_ragged_execute(void* plan, const float* pcm, float* out_real, float* out_imag,
+                                        float* out_mag);
+/* Graph launches this plan has issued (one per execute). */
+FFT_CFFI_API unsigned long long fftfree_ragged_launch_count(void* plan);
+FFT_CFFI_API void fftfree_ragged_free(void* plan);
+
 /* Test hook of the recovery coordinator (fft_cffi.cpp:954-982): runs the
  * host-side dropout / restore / split decisions for one batch of `frames`
  * frames, invoking the registered restore observer as the recovery path
