@@ -438,7 +438,40 @@ def measure_legs(ff, torch, stream, reps: int = 10):
     c.close()
     legs["autograd_stft_magnitude"] = measure_autograd(torch, stream, timed)
     legs["ragged_r2c_4096"] = measure_ragged(ff, torch, stream, timed)
+    legs["precision_c2c_n65536_b2048"] = measure_precision(ff, torch, stream, timed)
     return legs
+
+
+def measure_precision(ff, torch, stream, timed):
+    """C2C N=65536 (256 x 256 four-step) x 2048, re/im N(0,1) from seed 3:
+    the FP32 CUDA-core path against the split-FP16 tensor-core radix-16
+    variant (FFTFREE_TC16=1), each with its rel-L2 against an FP64 DFT of 8
+    transforms."""
+    import numpy as np
+
+    N, B = 65536, 2048
+    rng = np.random.default_rng(3)
+    z = rng.standard_normal((B, N, 2)).astype(np.float32)
+    x = torch.from_numpy(z).cuda()
+    y = torch.empty_like(x)
+    ref = np.fft.fft(z[:8, :, 0].astype(np.float64) + 1j * z[:8, :, 1].astype(np.float64), axis=1)
+    out = {}
+    for name, tc in (("fp32_cuda_core", "0"), ("split_fp16_tensor_core", "1")):
+        os.environ["FFTFREE_TC16"] = tc
+        c = ff.FftContext.full_v2(N, kernel=2)
+        c.set_stream(stream.cuda_stream)
+        c.set_async(True)
+        r = timed(lambda: c.execute_c2c(x, y, B), 16 * N * B)
+        torch.cuda.synchronize()
+        got = y[:8].cpu().numpy()
+        got = got[..., 0].astype(np.float64) + 1j * got[..., 1].astype(np.float64)
+        r["rel_l2_vs_fp64"] = float(f"{np.linalg.norm(got - ref) / np.linalg.norm(ref):.3e}")
+        out[name] = r
+        c.close()
+    os.environ.pop("FFTFREE_TC16", None)
+    out["kept"] = "split_fp16_tensor_core" if out["split_fp16_tensor_core"]["ms"] < out["fp32_cuda_core"]["ms"] \
+        else "fp32_cuda_core"
+    return out
 
 
 def measure_ragged(ff, torch, stream, timed):

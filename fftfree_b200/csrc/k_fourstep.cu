@@ -17,6 +17,7 @@
 #include <mutex>
 
 #include "fft_launch.cuh"
+#include "tc16.cuh"
 
 namespace ffb {
 
@@ -40,7 +41,25 @@ __host__ __device__ constexpr int cols_for() {
   return (S::T * FFTFREE_FOURSTEP_COLS <= 1024) ? FFTFREE_FOURSTEP_COLS : 1024 / S::T;
 }
 
-template <class S1, class IO>
+// The transform of each column / row group: the radix-R engine, or (TC, for
+// 256-point groups) the split-FP16 tensor-core DFT of tc16.cuh, one warp per
+// group tile.
+template <class S, bool TC>
+__device__ __forceinline__ void group_fft(float2 (&v)[S::R], int t, float2* smem, int group, int groups,
+                                          const Twiddles& tw) {
+  float2* tile = smem + group * tile_stride<S>();
+  if constexpr (TC && S::LOGM == 8) {
+    tile_write_natural<S>(v, t, tile);
+    __syncthreads();
+    for (int gg = threadIdx.x >> 5; gg < groups; gg += blockDim.x >> 5) tc_fft256(smem + gg * tile_stride<S>(), tw);
+    __syncthreads();
+    tile_read<S>(v, t, tile);
+  } else {
+    fft_engine<S>(v, t, tile, tw);
+  }
+}
+
+template <class S1, class IO, bool TC>
 __global__ void __launch_bounds__(S1::T * cols_for<S1>())
 k_four_a(IO io, float2* __restrict__ scratch, long long b0, int LN, Twiddles tw) {
   extern __shared__ float2 smem[];
@@ -57,7 +76,7 @@ k_four_a(IO io, float2* __restrict__ scratch, long long b0, int LN, Twiddles tw)
   float2 v[S1::R];
 #pragma unroll
   for (int i = 0; i < S1::R; ++i) v[i] = io.elem4(b, (long long)(t + i * T1) * N2 + n2);
-  fft_engine<S1>(v, t, smem + c * tile_stride<S1>(), tw);
+  group_fft<S1, TC>(v, t, smem, c, C, tw);
   float2* out = scratch + bl * ((long long)N1 * N2);
 #pragma unroll
   for (int i = 0; i < S1::R; ++i) {
@@ -66,7 +85,7 @@ k_four_a(IO io, float2* __restrict__ scratch, long long b0, int LN, Twiddles tw)
   }
 }
 
-template <class S2, class IO>
+template <class S2, class IO, bool TC>
 __global__ void __launch_bounds__(S2::T * cols_for<S2>())
 k_four_b(IO io, const float2* __restrict__ scratch, long long b0, int LN, Twiddles tw) {
   extern __shared__ float2 smem[];
@@ -83,7 +102,7 @@ k_four_b(IO io, const float2* __restrict__ scratch, long long b0, int LN, Twiddl
   float2 v[S2::R];
 #pragma unroll
   for (int i = 0; i < S2::R; ++i) v[i] = row[t + i * T2];
-  fft_engine<S2>(v, t, smem + g * tile_stride<S2>(), tw);
+  group_fft<S2, TC>(v, t, smem, g, C, tw);
   __syncthreads();  // the tiles are reused for staging
 #pragma unroll
   for (int i = 0; i < S2::R; ++i) smem[(t + i * T2) * (C + 1) + g] = v[i];
@@ -134,7 +153,7 @@ FourStepStreams& pipeline_streams() {
   return p;
 }
 
-template <int LN1, int LN2, class IO>
+template <int LN1, int LN2, class IO, bool TC = false>
 cudaError_t run_four(const IO& io, long long batch, float2* scratch, long long chunk, cudaStream_t st,
                      uint64_t* launches) {
   using S1 = SubSched<LN1>;
@@ -144,9 +163,9 @@ cudaError_t run_four(const IO& io, long long batch, float2* scratch, long long c
   const size_t sm1 = (size_t)C1 * tile_stride<S1>() * sizeof(float2);
   // pass B also stages its C2 x N2 results with a (C2 + 1) stride
   const size_t sm2 = std::max((size_t)C2 * tile_stride<S2>(), (size_t)S2::M * (C2 + 1)) * sizeof(float2);
-  cudaError_t e = set_smem<S1>((const void*)k_four_a<S1, IO>, sm1);
+  cudaError_t e = set_smem<S1>((const void*)k_four_a<S1, IO, TC>, sm1);
   if (e != cudaSuccess) return e;
-  e = set_smem<S2>((const void*)k_four_b<S2, IO>, sm2);
+  e = set_smem<S2>((const void*)k_four_b<S2, IO, TC>, sm2);
   if (e != cudaSuccess) return e;
   Twiddles tw{twiddle_pyramid(LN, st), twiddle_pass_tables(st)};
   const long long slot = chunk * (1LL << LN);  // complex points per scratch slot
@@ -169,12 +188,12 @@ cudaError_t run_four(const IO& io, long long batch, float2* scratch, long long c
     const long long ga = nb * ((1LL << LN2) / C1);
     const long long gb = nb * ((1LL << LN1) / C2);
     if (pipelined && i >= 2) cudaStreamWaitEvent(sa, p.done_b[sl], 0);
-    k_four_a<S1, IO><<<(unsigned)ga, S1::T * C1, sm1, sa>>>(io, buf, b0, LN, tw);
+    k_four_a<S1, IO, TC><<<(unsigned)ga, S1::T * C1, sm1, sa>>>(io, buf, b0, LN, tw);
     if (pipelined) {
       cudaEventRecord(p.done_a[sl], sa);
       cudaStreamWaitEvent(sb, p.done_a[sl], 0);
     }
-    k_four_b<S2, IO><<<(unsigned)gb, S2::T * C2, sm2, sb>>>(io, buf, b0, LN, tw);
+    k_four_b<S2, IO, TC><<<(unsigned)gb, S2::T * C2, sm2, sb>>>(io, buf, b0, LN, tw);
     if (pipelined) cudaEventRecord(p.done_b[sl], sb);
     if (launches) *launches += 2;
     e = cudaGetLastError();
@@ -190,17 +209,17 @@ cudaError_t run_four(const IO& io, long long batch, float2* scratch, long long c
   return cudaGetLastError();
 }
 
-template <class IO>
+template <class IO, bool TC = false>
 cudaError_t four_dispatch(const IO& io, int LN, long long batch, float2* scratch, long long chunk,
                           cudaStream_t st, uint64_t* l) {
   switch (LN) {
-    case 14: return run_four<7, 7, IO>(io, batch, scratch, chunk, st, l);
-    case 15: return run_four<8, 7, IO>(io, batch, scratch, chunk, st, l);
-    case 16: return run_four<8, 8, IO>(io, batch, scratch, chunk, st, l);
-    case 17: return run_four<9, 8, IO>(io, batch, scratch, chunk, st, l);
-    case 18: return run_four<9, 9, IO>(io, batch, scratch, chunk, st, l);
-    case 19: return run_four<10, 9, IO>(io, batch, scratch, chunk, st, l);
-    case 20: return run_four<10, 10, IO>(io, batch, scratch, chunk, st, l);
+    case 14: return run_four<7, 7, IO, TC>(io, batch, scratch, chunk, st, l);
+    case 15: return run_four<8, 7, IO, TC>(io, batch, scratch, chunk, st, l);
+    case 16: return run_four<8, 8, IO, TC>(io, batch, scratch, chunk, st, l);
+    case 17: return run_four<9, 8, IO, TC>(io, batch, scratch, chunk, st, l);
+    case 18: return run_four<9, 9, IO, TC>(io, batch, scratch, chunk, st, l);
+    case 19: return run_four<10, 9, IO, TC>(io, batch, scratch, chunk, st, l);
+    case 20: return run_four<10, 10, IO, TC>(io, batch, scratch, chunk, st, l);
     default: return cudaErrorInvalidValue;
   }
 }
@@ -234,9 +253,20 @@ cudaError_t launch_four_step_stft(const StftArgs& a, float2* scratch, size_t chu
   }
 }
 
+// FFTFREE_TC16=1 runs the 256-point groups of the C2C multi-pass transforms
+// (2^15 .. 2^17 points) on the tensor cores in split FP16 (tc16.cuh); off by
+// default: measured slower than the FP32 engine at this accuracy.
+bool tc16_requested() {
+  const char* e = std::getenv("FFTFREE_TC16");
+  return e && e[0] == '1';
+}
+
 cudaError_t launch_four_step_c2c(const C2cArgs& a, float2* scratch, size_t chunk, cudaStream_t s,
                                  uint64_t* launches) {
-  return four_dispatch(C2cIO{a}, ilog2i(a.N), a.batch, scratch, (long long)chunk, s, launches);
+  const int LN = ilog2i(a.N);
+  if (tc16_requested() && LN >= 15 && LN <= 17)
+    return four_dispatch<C2cIO, true>(C2cIO{a}, LN, a.batch, scratch, (long long)chunk, s, launches);
+  return four_dispatch(C2cIO{a}, LN, a.batch, scratch, (long long)chunk, s, launches);
 }
 
 cudaError_t launch_four_step_cplx(const CplxBatchArgs& a, float2* scratch, size_t chunk, cudaStream_t s,
