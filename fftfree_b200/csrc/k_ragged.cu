@@ -166,7 +166,7 @@ __device__ __forceinline__ void ragged_tile(const RaggedArgs& a, int4 tile, floa
 }
 
 template <int MODE>
-__global__ void __launch_bounds__(kBlock, 2) k_ragged(RaggedArgs a, Twiddles tw) {
+__global__ void __launch_bounds__(kBlock, 3) k_ragged(RaggedArgs a, Twiddles tw) {
   extern __shared__ float2 smem[];
   __shared__ int next;
   for (;;) {
