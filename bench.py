@@ -171,6 +171,8 @@ CASES = {
     "mag_phasor_n2048": "magnitude + unit phasor STFT N=W=2048 H=512, 64 x 262144 samples (autograd forward)",
     "grad_phasor_n2048": "magnitude STFT gradient from the saved phasor, N=W=2048 H=512, 64 x 262144",
     "grad_recompute_n2048": "magnitude STFT gradient with the spectrum recomputed, N=W=2048 H=512, 64 x 262144",
+    "c2c_n65536_b512": "C2C N=65536 x 512 complex64, four-step (two passes)",
+    "ragged_4096": "ragged batch: 4096 R2C signals, N = 2^e, e uniform in 6..16 (seed 2), one persistent launch",
 }
 
 
@@ -190,6 +192,22 @@ def run_case(args):
         c.set_stream(stream.cuda_stream)
         c.set_async(True)
         fn, nbytes = (lambda: c.execute_c2c(x, y, 8192)), 2 * x.numel() * 4
+    elif name == "c2c_n65536_b512":
+        x = torch.randn(512, 65536, 2, device="cuda", generator=g)
+        y = torch.empty_like(x)
+        c = ff.FftContext.full_v2(65536, kernel=2)
+        c.set_stream(stream.cuda_stream)
+        c.set_async(True)
+        fn, nbytes = (lambda: c.execute_c2c(x, y, 512)), 2 * x.numel() * 4
+    elif name == "ragged_4096":
+        import numpy as np
+        rng = np.random.default_rng(2)
+        sizes = [1 << int(v) for v in rng.integers(6, 17, 4096)]
+        pcm = torch.from_numpy(np.concatenate([rng.uniform(-1, 1, n) for n in sizes]).astype(np.float32)).cuda()
+        plan = ff.RaggedPlan(sizes)
+        plan.set_stream(stream.cuda_stream)
+        re, im, mg = (torch.empty(plan.bins, device="cuda") for _ in range(3))
+        fn, nbytes = (lambda: plan.execute(pcm, re, im, mg)), plan.samples * 4 + 3 * plan.bins * 4
     elif name == "stft_n1024_h256":
         L = 128 * 65536
         pcm = torch.rand(L, device="cuda", generator=g) * 2 - 1
