@@ -71,10 +71,12 @@ __device__ __forceinline__ float2 post_hook_m(float2 X, int k, int N, const Post
 __host__ __device__ inline int post_mode(const PostFlags& pf) { return pf.polar ? 2 : (pf.reduce ? 1 : 0); }
 
 // X / |X| for the magnitude gradient's saved phasor; 0 where |X| = 0, where
-// the gradient of |X| is taken as 0.
+// the gradient of |X| is taken as 0.  X * rsqrt(|X|^2) (a few ulp, far inside
+// the gradient's tolerance) in the range where |X|^2 is a normal float.
 __device__ __forceinline__ float2 unit_phasor(float2 X, float mag) {
   if (!(mag > 0.f)) return make_float2(0.f, 0.f);
-  const float r = 1.0f / mag;
+  const float s = fmaf(X.x, X.x, X.y * X.y);
+  const float r = (s > 1e-36f && s < 1e36f) ? rsqrtf(s) : 1.0f / mag;
   return make_float2(X.x * r, X.y * r);
 }
 
