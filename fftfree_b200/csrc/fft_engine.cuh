@@ -40,6 +40,12 @@ __device__ __forceinline__ float2 csub(float2 a, float2 b) {
 __device__ __forceinline__ float2 cmul(float2 a, float2 b) {
   return make_float2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
 }
+// a * b rounded term by term (no contraction into FMA): the same bits in
+// every kernel that inlines it, also when b is a compile-time constant
+__device__ __forceinline__ float2 cmul_rn(float2 a, float2 b) {
+  return make_float2(__fsub_rn(__fmul_rn(a.x, b.x), __fmul_rn(a.y, b.y)),
+                     __fadd_rn(__fmul_rn(a.x, b.y), __fmul_rn(a.y, b.x)));
+}
 __device__ __forceinline__ float2 cconj(float2 a) { return make_float2(a.x, -a.y); }
 __device__ __forceinline__ float2 cscale(float2 a, float s) { return __fmul2_rn(a, make_float2(s, s)); }
 // -i * a
@@ -127,6 +133,65 @@ __device__ __forceinline__ float2 w32(int m) {
     default: return w16(m >> 1);
   }
 }
+
+// exp(-2*pi*i*m/64) for odd m < 32
+__device__ __forceinline__ float2 w64_odd(int m) {
+  constexpr float c1 = 0.99518472667219688624f;  // cos(pi/32)
+  constexpr float s1 = 0.09801714032956060199f;  // sin(pi/32)
+  constexpr float c3 = 0.95694033573220886494f;  // cos(3pi/32)
+  constexpr float s3 = 0.29028467725446236764f;  // sin(3pi/32)
+  constexpr float c5 = 0.88192126434835502971f;  // cos(5pi/32)
+  constexpr float s5 = 0.47139673682599764856f;  // sin(5pi/32)
+  constexpr float c7 = 0.77301045336273696081f;  // cos(7pi/32)
+  constexpr float s7 = 0.63439328416364549822f;  // sin(7pi/32)
+  switch (m) {
+    case 1: return make_float2(c1, -s1);
+    case 3: return make_float2(c3, -s3);
+    case 5: return make_float2(c5, -s5);
+    case 7: return make_float2(c7, -s7);
+    case 9: return make_float2(s7, -c7);
+    case 11: return make_float2(s5, -c5);
+    case 13: return make_float2(s3, -c3);
+    case 15: return make_float2(s1, -c1);
+    case 17: return make_float2(-s1, -c1);
+    case 19: return make_float2(-s3, -c3);
+    case 21: return make_float2(-s5, -c5);
+    case 23: return make_float2(-s7, -c7);
+    case 25: return make_float2(-c7, -s7);
+    case 27: return make_float2(-c5, -s5);
+    case 29: return make_float2(-c3, -s3);
+    default: return make_float2(-c1, -s1);  // 31
+  }
+}
+
+// exp(-2*pi*i*m/64) for any m (a compile-time m folds to a constant)
+__device__ __forceinline__ float2 w64(int m) {
+  m &= 63;
+  const float sg = (m >= 32) ? -1.f : 1.f;  // w^(m + 32) = -w^m
+  m &= 31;
+  const float2 r = ((m & 1) == 0) ? w32(m >> 1) : w64_odd(m);
+  return make_float2(sg * r.x + 0.f, sg * r.y + 0.f);  // + 0: no negative zeros
+}
+
+// exp(-2 pi i m / L) for L = 2..64
+template <int L>
+__device__ __forceinline__ float2 wconst(int m) {
+  static_assert(L >= 1 && L <= 64 && (L & (L - 1)) == 0, "L a power of two up to 64");
+  return w64(m * (64 / L));
+}
+
+// Untangle / Hermitian twiddle w_N^(t + i T) of a transform of M = N/2
+// points held as v[i] = point t + i T: w_N^t (one load per thread) times
+// w_{2R}^i (a compile-time constant, since N / T = 2R), rounded term by term.
+template <class S>
+struct UntangleTw {
+  float2 wt;
+  __device__ __forceinline__ UntangleTw(const Twiddles& tw, int t)
+      : wt(__ldg(tw.pyr + ((2u << S::LOGM) - 1u) + t)) {}
+  __device__ __forceinline__ float2 operator()(int i) const {
+    return i == 0 ? wt : cmul_rn(wt, wconst<2 * S::R>(i));
+  }
+};
 
 // ---------------------------------------------------------------- small DFTs
 // Forward DFT of R points held in v[0 .. R-1], in place, natural order.
@@ -314,7 +379,17 @@ __device__ __forceinline__ void stockham_pass(float2 (&v)[S::R], int t, float2* 
   constexpr int LNS = S::LOGR0 + P * LR;
   constexpr int NS = 1 << LNS;
   const int k = t & (NS - 1);
-  if constexpr (LNS > 0) {
+  if constexpr (LNS > 0 && NS <= 4 && NS * R <= 64) {
+    // few distinct twiddles (k < NS): compile-time constants, chosen by k
+#pragma unroll
+    for (int r = 1; r < R; ++r) {
+      float2 w = make_float2(1.f, 0.f);
+#pragma unroll
+      for (int kk = 1; kk < NS; ++kk)
+        if (k == kk) w = wconst<NS * R>(r * kk);
+      v[r] = cmul_rn(v[r], w);
+    }
+  } else if constexpr (LNS > 0) {
     const float2* w = tw.pass + pass_table_offset(LR, LNS) + k;
 #pragma unroll
     for (int r = 1; r < R; ++r) v[r] = cmul(v[r], __ldg(w + (r - 1) * NS));

@@ -221,7 +221,7 @@ struct StftIO {
     if (bins == M + 1 && !a.inverse) {
       // Common STFT case (half spectrum, forward): bins 0..M, each written
       // once, no bounds or mirror logic.
-      const float2* w = tw.pyr + ((1 << LN) - 1) + t;
+      const UntangleTw<S> w(tw, t);
       float* pr = re + t;
       float* pi = im + t;
       float* pm = mg + t;
@@ -232,7 +232,7 @@ struct StftIO {
         const float2 E = make_float2(0.5f * (zk.x + zm.x), 0.5f * (zk.y - zm.y));
         const float2 D = make_float2(zk.x - zm.x, zk.y + zm.y);
         const float2 O = make_float2(0.5f * D.y, -0.5f * D.x);
-        float2 X = cadd(E, cmul(__ldg(w + i * T), O));
+        float2 X = cadd(E, cmul_rn(w(i), O));
         if (i == 0 && t == 0) X.y = 0.f;  // DC
         if constexpr (MODE >= 3) {
           const float m = cabs_fast(X.x, X.y);
@@ -468,7 +468,7 @@ struct C2rHalfIO {
       if (t == 0) sm[pidx(M)] = bin(re, im, M, true, cs);
     }
     GroupSync::sync<S>();
-    const float2* w = tw.pyr + ((1 << LN) - 1) + t;
+    const UntangleTw<S> w(tw, t);
 #pragma unroll
     for (int i = 0; i < R; ++i) {
       const int m = t + i * T;
@@ -477,7 +477,7 @@ struct C2rHalfIO {
         const float2 xm = sm[pidx(M - m)];
         const float2 E = make_float2(0.5f * (xk[i].x + xm.x), 0.5f * (xk[i].y - xm.y));
         const float2 D = make_float2(0.5f * (xk[i].x - xm.x), 0.5f * (xk[i].y + xm.y));
-        const float2 O = cmul(D, cconj(__ldg(w + i * T)));
+        const float2 O = cmul_rn(D, cconj(w(i)));
         z = make_float2(E.x - O.y, E.y + O.x);  // E + i O
       }
       v[i] = cconj(z);  // IDFT via conj . DFT . conj

@@ -124,7 +124,7 @@ __device__ __forceinline__ void grad_inverse(const MagGradArgs& a, const float2 
                                              float2 (&v)[S::R]) {
   constexpr int T = S::T, R = S::R, M = S::M;
   constexpr int LN = S::LOGM + 1;  // N = 2M
-  const float2* w = tw.pyr + ((1 << LN) - 1) + t;  // e^{-2 pi i m / N}, m = t + i*T
+  const UntangleTw<S> w(tw, t);  // e^{-2 pi i m / N}, m = t + i*T
   tile_write_natural<S>(y, t, sm);
   if (t == 0) sm[pidx(M)] = ynyq;
   GroupSync::sync<S>();
@@ -139,7 +139,7 @@ __device__ __forceinline__ void grad_inverse(const MagGradArgs& a, const float2 
     const float2 ym = sm[pidx(M - m)];
     const float2 E = make_float2(0.5f * (y[i].x + ym.x), 0.5f * (y[i].y - ym.y));
     const float2 D = make_float2(0.5f * (y[i].x - ym.x), 0.5f * (y[i].y + ym.y));
-    const float2 O = cmul(D, cconj(__ldg(w + i * T)));
+    const float2 O = cmul(D, cconj(w(i)));
     v[i] = make_float2(E.x - O.y, -(E.y + O.x));
   }
   GroupSync::sync<S>();  // the engine reuses the tile
@@ -169,7 +169,7 @@ __device__ __forceinline__ void frame_grad(const MagGradArgs& a, const float* pc
                                            bool ok, int t, float2* sm, const Twiddles& tw, float2 (&v)[S::R]) {
   constexpr int T = S::T, R = S::R, M = S::M;
   constexpr int LN = S::LOGM + 1;  // N = 2M
-  const float2* w = tw.pyr + ((1 << LN) - 1) + t;  // e^{-2 pi i k / N}, k = t + i*T
+  const UntangleTw<S> w(tw, t);  // e^{-2 pi i k / N}, k = t + i*T
   long long cnt;
   grad_load<S>(a, pcm, f, ok, t, v, &cnt);
   // upstream gradient of this frame's bins, fetched before the transform
@@ -192,7 +192,7 @@ __device__ __forceinline__ void frame_grad(const MagGradArgs& a, const float* pc
     const float2 E = make_float2(0.5f * (zk.x + zm.x), 0.5f * (zk.y - zm.y));
     const float2 D = make_float2(zk.x - zm.x, zk.y + zm.y);
     const float2 O = make_float2(0.5f * D.y, -0.5f * D.x);
-    float2 X = cadd(E, cmul(__ldg(w + i * T), O));
+    float2 X = cadd(E, cmul_rn(w(i), O));
     if (i == 0 && t == 0) {
       X.y = 0.f;  // DC is real
       const float2 V = mag_chain(X, gk[0]);
