@@ -389,6 +389,21 @@ __device__ __forceinline__ void stockham_pass(float2 (&v)[S::R], int t, float2* 
         if (k == kk) w = wconst<NS * R>(r * kk);
       v[r] = cmul_rn(v[r], w);
     }
+  } else if constexpr (LNS > 0 && (R == 8 || R == 16)) {
+    // w^r for r = 4a + b (0 < b < 4) as w^(4a) w^b: the table rows r = 1, 2,
+    // 3 and the multiples of 4 are loaded, the rest are one product away
+    const float2* w = tw.pass + pass_table_offset(LR, LNS) + k;
+    float2 wb[4], wa[R / 4];
+#pragma unroll
+    for (int b = 1; b < 4; ++b) wb[b] = __ldg(w + (b - 1) * NS);
+#pragma unroll
+    for (int a = 1; a < R / 4; ++a) wa[a] = __ldg(w + (4 * a - 1) * NS);
+#pragma unroll
+    for (int r = 1; r < R; ++r) {
+      const int a = r >> 2, b = r & 3;
+      const float2 wr = (a == 0) ? wb[b] : (b == 0 ? wa[a] : cmul_rn(wa[a], wb[b]));
+      v[r] = cmul(v[r], wr);
+    }
   } else if constexpr (LNS > 0) {
     const float2* w = tw.pass + pass_table_offset(LR, LNS) + k;
 #pragma unroll
