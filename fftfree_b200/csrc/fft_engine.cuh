@@ -28,6 +28,7 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <type_traits>
 #include <utility>
 
 namespace ffb {
@@ -389,9 +390,12 @@ __device__ __forceinline__ void stockham_pass(float2 (&v)[S::R], int t, float2* 
         if (k == kk) w = wconst<NS * R>(r * kk);
       v[r] = cmul_rn(v[r], w);
     }
-  } else if constexpr (LNS > 0 && (R == 8 || R == 16)) {
+  } else if constexpr (LNS > 0 && (R == 8 || R == 16) && std::is_same<Y, GroupSync>::value) {
     // w^r for r = 4a + b (0 < b < 4) as w^(4a) w^b: the table rows r = 1, 2,
-    // 3 and the multiples of 4 are loaded, the rest are one product away
+    // 3 and the multiples of 4 are loaded, the rest are one product away.
+    // Single-pass kernels only (per-transform barriers): B200 sweeps show it
+    // faster there (C2C N=4096 -5%) and slower in the block-synchronised
+    // multi-pass kernels (N=65536 +5%).
     const float2* w = tw.pass + pass_table_offset(LR, LNS) + k;
     float2 wb[4], wa[R / 4];
 #pragma unroll
