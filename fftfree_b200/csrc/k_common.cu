@@ -81,6 +81,38 @@ cudaError_t launch_ola(const OlaArgs& a, cudaStream_t s, uint64_t* launches) {
   return cudaGetLastError();
 }
 
+// ------------------------------------------------------------------ Griffin-Lim
+// phase_infer.hpp:190-207: out = |mag| e^{i arg(t)} per bin of the frames the
+// forward pass produced; with a half spectrum, the DC bin's imaginary part
+// and (even N) the Nyquist bin's are cleared.
+__global__ void k_gl_project(const float* __restrict__ mag, const float* __restrict__ tr,
+                             const float* __restrict__ ti, float* __restrict__ re, float* __restrict__ im,
+                             long long nbins, int bins, int half, int even_n) {
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < nbins;
+       i += (long long)gridDim.x * blockDim.x) {
+    const float ph = atan2f(__ldg(ti + i), __ldg(tr + i));
+    const float m = __ldg(mag + i);
+    float s, c;
+    sincosf(ph, &s, &c);
+    re[i] = m * c;
+    float v = m * s;
+    if (half) {
+      const int k = (int)(i % bins);
+      if (k == 0 || (even_n && bins > 1 && k == bins - 1)) v = 0.f;
+    }
+    im[i] = v;
+  }
+}
+
+cudaError_t launch_gl_project(const float* mag, const float* tr, const float* ti, float* re, float* im,
+                              long long nbins, int bins, int half, int even_n, cudaStream_t s) {
+  if (nbins <= 0) return cudaSuccess;
+  long long blocks = (nbins + 255) / 256;
+  if (blocks > 148 * 32) blocks = 148 * 32;
+  k_gl_project<<<(unsigned)blocks, 256, 0, s>>>(mag, tr, ti, re, im, nbins, bins, half, even_n);
+  return cudaGetLastError();
+}
+
 // ------------------------------------------------------------------ twiddles
 namespace {
 struct Pyramid {

@@ -117,6 +117,10 @@ cudaError_t launch_stft(const StftArgs& a, int logr, cudaStream_t s, uint64_t* l
 cudaError_t launch_c2c(const C2cArgs& a, int logr, cudaStream_t s, uint64_t* launches);
 cudaError_t launch_cplx_batch(const CplxBatchArgs& a, int logr, cudaStream_t s, uint64_t* launches);
 cudaError_t launch_ola(const OlaArgs& a, cudaStream_t s, uint64_t* launches);
+// Griffin-Lim projection: re + i im = mag e^{i atan2(ti, tr)} (half spectrum:
+// DC and, for even N, Nyquist imaginary parts cleared).
+cudaError_t launch_gl_project(const float* mag, const float* tr, const float* ti, float* re, float* im,
+                              long long nbins, int bins, int half, int even_n, cudaStream_t s);
 // Largest N (log2) of the magnitude-gradient kernel; 0 for unsupported.
 int max_mag_grad_log();
 cudaError_t launch_stft_mag_grad(const MagGradArgs& a, int logr, cudaStream_t s, uint64_t* launches);

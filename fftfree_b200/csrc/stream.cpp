@@ -2,16 +2,20 @@
 // inference: the reference's host-side drivers over the batched entry points
 // (fft_cffi.cpp:1342-1742, 2058-2248; phase_infer.hpp).  Every transform they
 // issue runs through the GPU entry points of abi.cpp.
+#include <cuda_runtime.h>
+
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
 #include <random>
+#include <stdexcept>
 #include <vector>
 
 #include "../../include/fft_cffi.h"
 #include "../../include/fftfree_b200.h"
 #include "context.h"
+#include "kernels.h"
 
 namespace ffb {
 namespace {
@@ -399,51 +403,99 @@ FFT_CFFI_API int fft_griffin_lim(void* ctx_forward, void* ctx_inverse, const flo
     const size_t total_bins = bins * frames;
     const size_t hp = (size_t)cfg_hop;
     const size_t ola_len = (frames - 1) * hp + plan_n;
-    std::vector<float> frame_pcm(frames * plan_n, 0.0f), ola(ola_len, 0.0f), w(ola_len, 0.0f);
-    std::vector<float> tr(total_bins), ti(total_bins), tm(total_bins);
     const int iters = (iterations > 0) ? iterations : 32;
+    // Initial phases as the reference draws them (phase_infer.hpp:128-138):
+    // std::mt19937 and a float uniform in [-pi, pi), on the host.
     const float kPi = 3.14159265358979323846f;
     std::mt19937 rng(seed ? seed : 0x47d7bfad);
     std::uniform_real_distribution<float> dist(-kPi, kPi);
+    // A device-resident magnitude is read back once for the initial spectra.
+    std::vector<float> mag_host;
+    const float* hmag = in_mag;
+    cudaPointerAttributes pa{};
+    if (cudaPointerGetAttributes(&pa, in_mag) == cudaSuccess && pa.type == cudaMemoryTypeDevice) {
+      mag_host.resize(total_bins);
+      if (cudaMemcpy(mag_host.data(), in_mag, total_bins * sizeof(float), cudaMemcpyDeviceToHost) != cudaSuccess)
+        return 0;
+      hmag = mag_host.data();
+    } else {
+      cudaGetLastError();
+    }
+    std::vector<float> re0(total_bins), im0(total_bins);
     for (size_t i = 0; i < total_bins; ++i) {
       const float a = dist(rng);
-      out_real[i] = in_mag[i] * std::cos(a);
-      out_imag[i] = in_mag[i] * std::sin(a);
+      re0[i] = hmag[i] * std::cos(a);
+      im0[i] = hmag[i] * std::sin(a);
     }
+    // The iterations run on the device (phase_infer.hpp:140-208): the inverse
+    // batch, the count-normalised overlap-add, the forward STFT and the phase
+    // projection, with every intermediate in device memory.
+    int prev = -1;
+    cudaGetDevice(&prev);
+    if (prev != fc->device) cudaSetDevice(fc->device);
+    struct Restore {
+      int dev;
+      ~Restore() {
+        if (dev >= 0) cudaSetDevice(dev);
+      }
+    } restore{prev != fc->device ? prev : -1};
+    DevBuf d_mag, d_re, d_im, d_frames, d_ola, d_tr, d_ti, d_tm;
+    const size_t fb = total_bins * sizeof(float);
+    float* mag = static_cast<float*>(d_mag.get(fb));
+    float* re = static_cast<float*>(d_re.get(fb));
+    float* im = static_cast<float*>(d_im.get(fb));
+    float* tr = static_cast<float*>(d_tr.get(fb));
+    float* ti = static_cast<float*>(d_ti.get(fb));
+    float* tm = static_cast<float*>(d_tm.get(fb));
+    float* frame_pcm = static_cast<float*>(d_frames.get(frames * plan_n * sizeof(float)));
+    const size_t ola_cap = std::max(ola_len, frames * plan_n);
+    float* ola = static_cast<float*>(d_ola.get(ola_cap * sizeof(float)));
+    cudaStream_t st = fc->stream;
+    auto ok = [](cudaError_t e) {
+      if (e != cudaSuccess) throw std::runtime_error("cuda");
+    };
+    ok(cudaMemcpyAsync(mag, in_mag, fb, cudaMemcpyDefault, st));
+    ok(cudaMemcpyAsync(re, re0.data(), fb, cudaMemcpyHostToDevice, st));
+    ok(cudaMemcpyAsync(im, im0.data(), fb, cudaMemcpyHostToDevice, st));
+    ok(cudaStreamSynchronize(st));
+    // The reference refines out_real/out_imag in place, so a failed pass
+    // leaves the spectra of the last completed one there.
+    auto flush = [&]() {
+      ok(cudaMemcpyAsync(out_real, re, fb, cudaMemcpyDefault, st));
+      ok(cudaMemcpyAsync(out_imag, im, fb, cudaMemcpyDefault, st));
+      ok(cudaStreamSynchronize(st));
+    };
     for (int it = 0; it < iters; ++it) {
-      const size_t pr = fft_execute_complex_batched(ctx_inverse, out_real, out_imag, frames,
-                                                    frame_pcm.data(), pad_mode, 0, frames);
-      if (pr == 0) return 0;
-      std::fill(ola.begin(), ola.end(), 0.0f);
-      std::fill(w.begin(), w.end(), 0.0f);
+      const size_t pr = fft_execute_complex_batched(ctx_inverse, re, im, frames, frame_pcm, pad_mode, 0, frames);
+      if (pr == 0) {
+        flush();
+        return 0;
+      }
+      ok(cudaStreamSynchronize(ic->stream));
       const size_t uf = std::min(pr, frames);
-      for (size_t f = 0; f < uf; ++f) {
-        const float* src = frame_pcm.data() + f * plan_n;
-        const size_t start = f * hp;
-        if (start + plan_n > ola_len) break;
-        for (size_t n = 0; n < plan_n; ++n) {
-          ola[start + n] += src[n];
-          w[start + n] += 1.0f;
-        }
+      ok(cudaMemsetAsync(ola, 0, ola_cap * sizeof(float), st));
+      OlaArgs o{};
+      o.frames_buf = frame_pcm;
+      o.frames = (long long)uf;
+      o.N = (int)plan_n;
+      o.H = (int)hp;
+      o.cola = 1;  // divide by the number of frames covering the sample
+      o.weight = nullptr;
+      o.out = ola;
+      ok(launch_ola(o, st, &fc->launches));
+      ok(cudaStreamSynchronize(st));
+      const size_t ff = fft_execute_batched(ctx_forward, ola, ola_len, tr, ti, tm, pad_mode, 0, frames);
+      if (ff == 0) {
+        flush();
+        return 0;
       }
-      for (size_t n = 0; n < ola_len; ++n)
-        if (w[n] > 0.0f) ola[n] /= w[n];
-      const size_t ff = fft_execute_batched(ctx_forward, ola.data(), ola_len, tr.data(), ti.data(),
-                                            tm.data(), pad_mode, 0, frames);
-      if (ff == 0) return 0;
+      ok(cudaStreamSynchronize(fc->stream));
       const size_t uff = std::min(ff, frames);
-      for (size_t i = 0; i < uff * bins; ++i) {
-        const float ph = std::atan2(ti[i], tr[i]);
-        out_real[i] = in_mag[i] * std::cos(ph);
-        out_imag[i] = in_mag[i] * std::sin(ph);
-      }
-      if (half) {
-        for (size_t f = 0; f < uff; ++f) {
-          out_imag[f * bins] = 0.0f;
-          if ((plan_n & 1) == 0 && bins > 1) out_imag[f * bins + bins - 1] = 0.0f;
-        }
-      }
+      ok(launch_gl_project(mag, tr, ti, re, im, (long long)(uff * bins), (int)bins, half ? 1 : 0,
+                           (plan_n & 1) == 0 ? 1 : 0, st));
+      ok(cudaStreamSynchronize(st));
     }
+    flush();
     return 1;
   } catch (...) {
     return 0;
