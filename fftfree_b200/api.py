@@ -99,6 +99,8 @@ _SIGS = [
     ("fftfree_device_available", ctypes.c_int, []),
     ("fftfree_execute_complex_batched_noalloc", ctypes.c_size_t, [ctypes.c_void_p, c_float_p, c_float_p,
                                                                    ctypes.c_size_t, c_float_p, ctypes.c_size_t]),
+    ("fftfree_execute_2d", ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, c_float_p, c_float_p, ctypes.c_size_t,
+                                          ctypes.c_size_t, ctypes.c_size_t]),
     ("fftfree_stft_magnitude", ctypes.c_size_t, [ctypes.c_void_p, c_float_p, ctypes.c_size_t, ctypes.c_size_t,
                                                  c_float_p, ctypes.c_size_t]),
     ("fftfree_stft_magnitude_backward", ctypes.c_size_t, [ctypes.c_void_p, c_float_p, ctypes.c_size_t,
@@ -325,6 +327,15 @@ class RaggedPlan:
             self.close()
         except Exception:
             pass
+
+
+def execute_2d(ctx_axis0: "FftContext", ctx_axis1: "FftContext", x, out, rows: int, cols: int,
+               batch: int = 1) -> int:
+    """2-D transform of ``batch`` column-major rows x cols complex matrices
+    (eigen_fft.hpp:3177-3215): ctx_axis0 (N = rows) over the columns, then
+    ctx_axis1 (N = cols) over the rows.  ``x`` / ``out`` hold interleaved
+    complex float32 (host or CUDA), matrix after matrix; they may alias."""
+    return int(lib().fftfree_execute_2d(ctx_axis0.handle, ctx_axis1.handle, _fp(x), _fp(out), rows, cols, batch))
 
 
 def device_available() -> bool:

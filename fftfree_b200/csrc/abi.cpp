@@ -997,6 +997,82 @@ FFT_CFFI_API int fft_config_window_custom(void* handle, const float* analysis_wi
 }
 
 // ------------------------------------------------------------------ extensions
+// The context's C2C plan flags over `batch` contiguous lines of N points.
+static C2cArgs c2c_args(const FftContext* c, const float* in, float* out, size_t batch) {
+  C2cArgs a{};
+  a.in = reinterpret_cast<const float2*>(in);
+  a.out = reinterpret_cast<float2*>(out);
+  a.batch = (long long)batch;
+  a.N = c->N;
+  const int m = c->eff_transform();
+  a.pre = c->stockham() ? 0 : (m == 1 ? 1 : ((m == 2 && c->half_spectrum) ? 2 : 0));
+  a.polar_in = c->store_polar ? 1 : 0;
+  a.inverse = c->inverse ? 1 : 0;
+  a.pf = c->post_flags();
+  return a;
+}
+
+// Contiguous lines: single pass, or the multi-pass kernels with the
+// context's scratch.
+static void run_c2c_lines(FftContext* c, const C2cArgs& a, cudaStream_t s) {
+  if (single_pass(c->N, false)) {
+    FFB_CHECK(launch_c2c(a, c->logr_req, s, &c->launches));
+  } else {
+    size_t chunk = 0;
+    float2* scratch = scratch_for(c, c->N, a.batch, &chunk);
+    FFB_CHECK(launch_four_step_c2c(a, scratch, chunk, s, &c->launches));
+  }
+}
+
+FFT_CFFI_API int fftfree_execute_2d(void* ctx_axis0, void* ctx_axis1, const float* in, float* out, size_t rows,
+                                    size_t cols, size_t batch) {
+  // eigen_fft.hpp:3177-3215
+  FftContext* c0 = as_ctx(ctx_axis0);
+  FftContext* c1 = as_ctx(ctx_axis1);
+  if (!c0 || !c1 || !in || !out || rows == 0 || cols == 0 || batch == 0) return 0;
+  if ((size_t)c0->N != rows || (size_t)c1->N != cols) return 0;
+  if (c0->device != c1->device) return 0;
+  try {
+    std::unique_lock<std::recursive_mutex> l0(c0->mu, std::defer_lock), l1(c1->mu, std::defer_lock);
+    if (c0 == c1) {
+      l0.lock();
+    } else {
+      std::lock(l0, l1);
+    }
+    DeviceGuard g(c0->device);
+    cudaStream_t s = c0->stream;
+    const size_t n = batch * rows * cols * 2;
+    const bool in_host = !is_device_ptr(in);
+    OutTarget o = stage_out(c0->d_out0, out, n);
+    const float* d_in = stage_in(c0, c0->d_in0, in, n);
+    // axis 0: the columns are contiguous lines of `rows` points
+    run_c2c_lines(c0, c2c_args(c0, d_in, o.dev, batch * cols), s);
+    // axis 1: row r of matrix m is the line of `cols` points r + j * rows
+    C2cArgs a1 = c2c_args(c1, o.dev, o.dev, batch * rows);
+    if (ilog2(cols) <= max_strided_log()) {
+      StridedLinesArgs sl{a1, (long long)rows};
+      FFB_CHECK(launch_c2c_strided(sl, c1->logr_req, s, &c1->launches));
+    } else {
+      // lines beyond one pass: transpose, multi-pass over contiguous rows,
+      // transpose back (the reference's own route)
+      float2* t = static_cast<float2*>(c0->d_t2d.get(n * sizeof(float)));
+      float2* d = reinterpret_cast<float2*>(o.dev);
+      FFB_CHECK(launch_transpose(d, t, (long long)rows, (long long)cols, (long long)batch, s, &c0->launches));
+      a1.in = t;
+      a1.out = t;
+      size_t chunk = 0;
+      float2* scratch = scratch_for(c1, c1->N, a1.batch, &chunk);
+      FFB_CHECK(launch_four_step_c2c(a1, scratch, chunk, s, &c1->launches));
+      FFB_CHECK(launch_transpose(t, d, (long long)cols, (long long)rows, (long long)batch, s, &c0->launches));
+    }
+    finish_out(c0, o);
+    finish_call(c0, in_host || o.host);
+    return 1;
+  } catch (...) {
+    return 0;
+  }
+}
+
 FFT_CFFI_API int fftfree_execute_c2c(void* handle, const float* in, float* out, size_t batch) {
   FftContext* c = as_ctx(handle);
   if (!c || !in || !out || batch == 0) return 0;
@@ -1012,16 +1088,7 @@ FFT_CFFI_API int fftfree_execute_c2c(void* handle, const float* in, float* out, 
                            : 1;
     const float* d_in = (chunks > 1 && in_host) ? static_cast<const float*>(c->d_in0.get(n * sizeof(float)))
                                                 : stage_in(c, c->d_in0, in, n);
-    C2cArgs a{};
-    a.in = reinterpret_cast<const float2*>(d_in);
-    a.out = reinterpret_cast<float2*>(o.dev);
-    a.batch = (long long)batch;
-    a.N = c->N;
-    const int m = c->eff_transform();
-    a.pre = c->stockham() ? 0 : (m == 1 ? 1 : ((m == 2 && c->half_spectrum) ? 2 : 0));
-    a.polar_in = c->store_polar ? 1 : 0;
-    a.inverse = c->inverse ? 1 : 0;
-    a.pf = c->post_flags();
+    C2cArgs a = c2c_args(c, d_in, o.dev, batch);
     if (chunks > 1) {
       const size_t per = (batch + chunks - 1) / chunks, row = (size_t)c->N * 2;
       auto rows = [&](int i, size_t* r0, size_t* r1) {
@@ -1053,13 +1120,7 @@ FFT_CFFI_API int fftfree_execute_c2c(void* handle, const float* in, float* out, 
       finish_call(c, true);
       return 1;
     }
-    if (single_pass(c->N, false)) {
-      FFB_CHECK(launch_c2c(a, c->logr_req, c->stream, &c->launches));
-    } else {
-      size_t chunk = 0;
-      float2* scratch = scratch_for(c, c->N, (long long)batch, &chunk);
-      FFB_CHECK(launch_four_step_c2c(a, scratch, chunk, c->stream, &c->launches));
-    }
+    run_c2c_lines(c, a, c->stream);
     finish_out(c, o);
     finish_call(c, any_host);
     return 1;

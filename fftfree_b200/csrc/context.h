@@ -70,6 +70,7 @@ struct FftContext {
   DevBuf d_in0, d_in1, d_out0, d_out1, d_out2, d_frames;
   DevBuf d_meta_tw;  // reference float twiddle table for the metadata path
   DevBuf d_scratch;  // multi-pass intermediate chunk
+  DevBuf d_t2d;      // transposed matrices of a 2-D transform with long rows
   // host-buffer pipeline (abi.cpp): upload / download streams and events
   cudaStream_t up_stream = nullptr, down_stream = nullptr;
   std::vector<cudaEvent_t> pipe_events;

@@ -279,25 +279,32 @@ struct StftIO {
 };
 
 // ------------------------------------------------------------------ C2C IO
+// Element n of a C2C line after the Cooley-Tukey pre-hook; at(m) fetches
+// the line's raw element m (contiguous or strided lines).
+template <class At>
+__device__ __forceinline__ float2 c2c_pre_elem(const C2cArgs& a, const At& at, int n) {
+  if (a.pre == 1) {  // eigen_fft.hpp:2493-2502
+    float2 u = at(n);
+    u.y = 0.f;
+    return u;
+  }
+  if (a.pre == 2) {  // eigen_fft.hpp:2505-2531
+    int m = n;
+    bool cj = false;
+    if (m > (a.N >> 1)) { m = a.N - m; cj = true; }
+    float2 u = at(m);
+    if (a.polar_in) u = polar_to_complex(u);
+    if (m == 0 || m == (a.N >> 1)) u.y = 0.f;
+    return cj ? cconj(u) : u;
+  }
+  return at(n);
+}
+
 struct C2cIO {
   C2cArgs a;
 
   __device__ __forceinline__ float2 elem(const float2* col, int n) const {
-    if (a.pre == 1) {  // eigen_fft.hpp:2493-2502
-      float2 u = col[n];
-      u.y = 0.f;
-      return u;
-    }
-    if (a.pre == 2) {  // eigen_fft.hpp:2505-2531
-      int m = n;
-      bool cj = false;
-      if (m > (a.N >> 1)) { m = a.N - m; cj = true; }
-      float2 u = col[m];
-      if (a.polar_in) u = polar_to_complex(u);
-      if (m == 0 || m == (a.N >> 1)) u.y = 0.f;
-      return cj ? cconj(u) : u;
-    }
-    return col[n];
+    return c2c_pre_elem(a, [col](int m) { return col[m]; }, n);
   }
 
   __device__ __forceinline__ float2 elem4(long long b, long long n) const {

@@ -115,6 +115,20 @@ int max_single_pass_log();
 // incremented by the number of kernels enqueued.
 cudaError_t launch_stft(const StftArgs& a, int logr, cudaStream_t s, uint64_t* launches);
 cudaError_t launch_c2c(const C2cArgs& a, int logr, cudaStream_t s, uint64_t* launches);
+
+// Second axis of a 2-D transform: C2C lines whose elements are `rows`
+// complex values apart in column-major rows x c.N matrices; line l is row
+// (l % rows) of matrix (l / rows), c.batch lines in all.  Single pass, c.N up
+// to 2^max_strided_log().  In place (c.in == c.out) is allowed.
+struct StridedLinesArgs {
+  C2cArgs c;
+  long long rows;
+};
+int max_strided_log();
+cudaError_t launch_c2c_strided(const StridedLinesArgs& a, int logr, cudaStream_t s, uint64_t* launches);
+// Column-major rows x cols -> cols x rows, `batch` matrices back to back.
+cudaError_t launch_transpose(const float2* in, float2* out, long long rows, long long cols, long long batch,
+                             cudaStream_t s, uint64_t* launches);
 cudaError_t launch_cplx_batch(const CplxBatchArgs& a, int logr, cudaStream_t s, uint64_t* launches);
 cudaError_t launch_ola(const OlaArgs& a, cudaStream_t s, uint64_t* launches);
 // Griffin-Lim projection: re + i im = mag e^{i atan2(ti, tr)} (half spectrum:

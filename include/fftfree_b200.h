@@ -24,6 +24,17 @@ extern "C" {
  * Returns 1 on success. */
 FFT_CFFI_API int fftfree_execute_c2c(void* handle, const float* in, float* out, size_t batch);
 
+/* 2-D transform of `batch` column-major rows x cols complex matrices --
+ * eigfft::fft_inplace_2d (eigen_fft.hpp:3177-3215): the plan of ctx_axis0
+ * (N = rows) over every column, then the plan of ctx_axis1 (N = cols) over
+ * every row, each with its context's flags (direction, 1/N on inverse,
+ * hooks).  `in` / `out` hold batch * rows * cols interleaved complex floats,
+ * matrix after matrix; they may alias (the reference works in place).
+ * Returns 0 when a context's N does not match its axis (the reference throws
+ * std::invalid_argument there), 1 on success.  Runs on ctx_axis0's stream. */
+FFT_CFFI_API int fftfree_execute_2d(void* ctx_axis0, void* ctx_axis1, const float* in, float* out, size_t rows,
+                                    size_t cols, size_t batch);
+
 /* One metadata request: the fields of eigfft::MetadataRequest
  * (eigen_fft.hpp:1496-1501); `buffer` holds `count` interleaved complex
  * floats.  Kinds are eigfft::MetadataKind ordinals (eigen_fft.hpp:1477-1491):

@@ -199,3 +199,21 @@ class OracleContext:
         ok = lib().oracle_fft_columns(ctypes.byref(c), X.view(np.float32).ctypes.data_as(
             ctypes.POINTER(ctypes.c_float)), B, arr, len(reqs), threads)
         return bool(ok), X, bufs
+
+
+def fft_2d(ctx_axis0: OracleContext, ctx_axis1: OracleContext, X: np.ndarray, threads: int = 1):
+    """fft_inplace_2d (eigen_fft.hpp:3177-3215).  X: (batch, cols, rows)
+    complex64 -- batch column-major rows x cols matrices, column c of matrix
+    b is X[b, c].  The axis-0 plan runs over every column, the tiled transpose
+    (eigen_fft.hpp:2448-2472, a pure data move) makes every row contiguous,
+    the axis-1 plan runs over them and the transpose moves them back.
+    Returns (ok, X_out) with X's shape."""
+    X = np.ascontiguousarray(X, dtype=np.complex64)
+    B, C, R = X.shape
+    if ctx_axis0.N != R or ctx_axis1.N != C:
+        return False, X
+    ok0, Y, _ = ctx_axis0.fft_columns(X.reshape(B * C, R), threads=threads)
+    Yt = np.ascontiguousarray(Y.reshape(B, C, R).transpose(0, 2, 1)).reshape(B * R, C)
+    ok1, Z, _ = ctx_axis1.fft_columns(Yt, threads=threads)
+    out = np.ascontiguousarray(Z.reshape(B, R, C).transpose(0, 2, 1))
+    return bool(ok0 and ok1), out
