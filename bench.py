@@ -173,6 +173,7 @@ CASES = {
     "grad_recompute_n2048": "magnitude STFT gradient with the spectrum recomputed, N=W=2048 H=512, 64 x 262144",
     "c2c_n65536_b512": "C2C N=65536 x 512 complex64, four-step (two passes)",
     "ragged_4096": "ragged batch: 4096 R2C signals, N = 2^e, e uniform in 6..16 (seed 2), one persistent launch",
+    "fft2d_4096x4096_b4": "2-D C2C of 4 column-major 4096 x 4096 complex64 matrices (column pass + strided row pass)",
 }
 
 
@@ -199,6 +200,14 @@ def run_case(args):
         c.set_stream(stream.cuda_stream)
         c.set_async(True)
         fn, nbytes = (lambda: c.execute_c2c(x, y, 512)), 2 * x.numel() * 4
+    elif name == "fft2d_4096x4096_b4":
+        x = torch.randn(4 * 4096 * 4096 * 2, device="cuda", generator=g)
+        y = torch.empty_like(x)
+        c = ff.FftContext.full_v2(4096, kernel=2)
+        c1 = ff.FftContext.full_v2(4096, kernel=2)
+        c.set_stream(stream.cuda_stream)
+        c.set_async(True)
+        fn, nbytes = (lambda: ff.execute_2d(c, c1, x, y, 4096, 4096, 4)), 2 * x.numel() * 4
     elif name == "ragged_4096":
         import numpy as np
         rng = np.random.default_rng(2)
@@ -454,6 +463,22 @@ def measure_legs(ff, torch, stream, reps: int = 10):
     legs["stft_r2c_n1024_h256_long_signal"]["frames_per_s"] = round(
         frames / (legs["stft_r2c_n1024_h256_long_signal"]["ms"] * 1e-3), 1)
     c.close()
+    # 2-D: 4 column-major 4096 x 4096 complex64 matrices, forward on both
+    # axes (columns by the batched kernel, rows by the strided one)
+    R2, B2 = 4096, 4
+    x2 = torch.randn(B2 * R2 * R2 * 2, device="cuda", generator=g)
+    y2 = torch.empty_like(x2)
+    c0 = ff.FftContext.full_v2(R2, kernel=2)
+    c1 = ff.FftContext.full_v2(R2, kernel=2)
+    c0.set_stream(stream.cuda_stream)
+    c0.set_async(True)
+    leg = timed(lambda: ff.execute_2d(c0, c1, x2, y2, R2, R2, B2), 2 * x2.numel() * 4)
+    # two passes are the least any out-of-cache 2-D transform moves
+    leg["two_pass_GB/s"] = round(4 * x2.numel() * 4 / (leg["ms"] * 1e-3) / 1e9, 1)
+    legs["fft2d_c2c_4096x4096_b4"] = leg
+    c0.close()
+    c1.close()
+    del x2, y2
     legs["autograd_stft_magnitude"] = measure_autograd(torch, stream, timed)
     legs["ragged_r2c_4096"] = measure_ragged(ff, torch, stream, timed)
     legs["precision_c2c_n65536_b2048"] = measure_precision(ff, torch, stream, timed)

@@ -325,6 +325,18 @@ struct Sched {
 // are the consecutive S::T-thread slices; at most 4 of them here), or the
 // block barrier when one transform is the whole block.
 struct BlockSync {
+  static constexpr bool kSplitTwiddles = false;  // pass twiddles: full table loads
+  template <class S>
+  __device__ __forceinline__ static void sync() {
+    __syncthreads();
+  }
+};
+
+// Block barriers for kernels whose transforms are interleaved across the
+// lanes of a block, with the twiddle arithmetic of the single-pass kernels
+// (bit-identical results to GroupSync engines).
+struct LaneBlockSync {
+  static constexpr bool kSplitTwiddles = true;
   template <class S>
   __device__ __forceinline__ static void sync() {
     __syncthreads();
@@ -332,6 +344,7 @@ struct BlockSync {
 };
 
 struct GroupSync {
+  static constexpr bool kSplitTwiddles = true;  // rows 1..3 and multiples of 4 loaded, the rest products
   template <class S>
   __device__ __forceinline__ static void sync() {
     if constexpr (S::T <= 32) {
@@ -390,7 +403,7 @@ __device__ __forceinline__ void stockham_pass(float2 (&v)[S::R], int t, float2* 
         if (k == kk) w = wconst<NS * R>(r * kk);
       v[r] = cmul_rn(v[r], w);
     }
-  } else if constexpr (LNS > 0 && (R == 8 || R == 16) && std::is_same<Y, GroupSync>::value) {
+  } else if constexpr (LNS > 0 && (R == 8 || R == 16) && Y::kSplitTwiddles) {
     // w^r for r = 4a + b (0 < b < 4) as w^(4a) w^b: the table rows r = 1, 2,
     // 3 and the multiples of 4 are loaded, the rest are one product away.
     // Single-pass kernels only (per-transform barriers): B200 sweeps show it

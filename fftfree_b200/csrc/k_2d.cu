@@ -5,29 +5,29 @@
 // The reference transposes the matrix into scratch, transforms the now
 // contiguous rows and transposes back (three passes over the matrix).  Here
 // one kernel does it in a single read and a single write: a block owns G
-// adjacent lines (adjacent rows of one matrix), gathers them into shared
-// memory with consecutive threads on consecutive lines -- every warp reads
-// whole 32-byte sectors -- runs the register-resident engine on each line
-// and scatters the result the same way.  Lines longer than the single-pass
-// engine (cols > 2^13) take the transpose / multi-pass / transpose route.
+// adjacent lines (adjacent rows of one matrix) and thread x works on line
+// x % G as engine thread x / G, so consecutive threads load and store
+// consecutive lines -- adjacent addresses, whole 32-byte sectors for G >= 4
+// -- straight between HBM and registers; shared memory only carries the
+// engine's exchanges.  Lines longer than the single-pass engine
+// (cols > 2^13) take the transpose / multi-pass / transpose route.
+#include <cstdlib>
+
 #include "fft_launch.cuh"
 
 namespace ffb {
 
-template <class S>
+template <class S, int WANT = 4>
 struct LinesLaunch {
-  // group stride (float2) with the bank offset that keeps the gather and
-  // scatter of G lines x (32 / G) elements per warp free of bank conflicts
+  // group stride (float2): the G groups of a half-warp land on disjoint banks
   static constexpr int gstride(int g) {
     const int res = g >= 16 ? 1 : 16 / g;
     return S::SMEM + (((res - S::SMEM % 16) % 16) + 16) % 16;
   }
-  static constexpr size_t bytes(int g) {
-    return (size_t)g * gstride(g) * sizeof(float2) + (size_t)g * sizeof(long long);
-  }
+  static constexpr size_t bytes(int g) { return (size_t)g * gstride(g) * sizeof(float2); }
   static constexpr int pick() {
     int g = (S::T >= 256) ? 1 : 256 / S::T;
-    const int want = (1024 / S::T < 4) ? 1024 / S::T : 4;  // >= 4 lines: whole sectors
+    const int want = (1024 / S::T < WANT) ? 1024 / S::T : WANT;  // >= 4 lines: whole sectors
     if (g < want) g = want;
     while (g > 1 && bytes(g) > 200 * 1024) g >>= 1;
     return g;
@@ -38,78 +38,90 @@ struct LinesLaunch {
   static constexpr size_t SMEM_BYTES = bytes(G);
 };
 
-template <class S>
-__global__ void __launch_bounds__(LinesLaunch<S>::BLOCK) k_fft_strided(StridedLinesArgs a, Twiddles tw) {
-  using L = LinesLaunch<S>;
+template <class S, int WANT>
+__global__ void __launch_bounds__(LinesLaunch<S, WANT>::BLOCK) k_fft_strided(StridedLinesArgs a, Twiddles tw) {
+  using L = LinesLaunch<S, WANT>;
   extern __shared__ float2 smem[];
-  constexpr int T = S::T, M = S::M, G = L::G, GS = L::GS, BLOCK = L::BLOCK;
+  constexpr int T = S::T, M = S::M, G = L::G, GS = L::GS;
   static_assert((G & (G - 1)) == 0, "lines per block: a power of two");
-  long long* off = reinterpret_cast<long long*>(smem + G * GS);
-  const int g = threadIdx.x / T;
-  const int t = threadIdx.x - g * T;
-  const long long l0 = (long long)blockIdx.x * G;
-  if (threadIdx.x < G) {
-    const long long l = l0 + threadIdx.x;
-    off[threadIdx.x] = (l < a.c.batch) ? (l / a.rows) * a.rows * (long long)M + (l % a.rows) : -1LL;
-  }
-  __syncthreads();
-  // gather: consecutive threads read consecutive lines (adjacent addresses)
-  const float sy = a.c.inverse ? -1.f : 1.f;  // inverse = conj . forward . conj
+  const int g = threadIdx.x & (G - 1);
+  const int t = threadIdx.x / G;
+  const long long l = (long long)blockIdx.x * G + g;
+  const bool live = l < a.c.batch;
   const long long st = a.rows;
-  for (int idx = threadIdx.x; idx < G * M; idx += BLOCK) {
-    const int gg = idx & (G - 1), n = idx / G;
-    const long long o = off[gg];
-    float2 u = make_float2(0.f, 0.f);
-    if (o >= 0) {
-      const float2* p = a.c.in + o;
-      u = c2c_pre_elem(a.c, [p, st](int m) { return p[(long long)m * st]; }, n);
-      u.y *= sy;
-    }
-    smem[gg * GS + pidx(n)] = u;
-  }
-  __syncthreads();
-  float2* sm = smem + g * GS;
+  const long long o = live ? (l / st) * st * (long long)M + (l % st) : 0;
   float2 v[S::R];
-  tile_read<S>(v, t, sm);
-  __syncthreads();
-  fft_engine<S, GroupSync>(v, t, sm, tw);
-  __syncthreads();
+  // inverse = conj . forward . conj
+  const float2 sg_in = make_float2(1.f, a.c.inverse ? -1.f : 1.f);
+  if (a.c.pre == 0) {
+    const float2* p = a.c.in + o;
+#pragma unroll
+    for (int i = 0; i < S::R; ++i)
+      v[i] = live ? __fmul2_rn(__ldcg(p + (long long)(t + i * T) * st), sg_in) : make_float2(0.f, 0.f);
+  } else {
+    const float2* p = a.c.in + o;
+    const auto at = [p, st](int m) { return __ldcg(p + (long long)m * st); };
+#pragma unroll
+    for (int i = 0; i < S::R; ++i)
+      v[i] = live ? __fmul2_rn(c2c_pre_elem(a.c, at, t + i * T), sg_in) : make_float2(0.f, 0.f);
+  }
+  // the groups of a block are interleaved across lanes: block barriers
+  fft_engine<S, LaneBlockSync>(v, t, smem + g * GS, tw);
+  if (!live) return;
   const float sc = a.c.inverse ? 1.0f / (float)M : 1.0f;
   const float2 sg = make_float2(sc, a.c.inverse ? -sc : sc);
+  float2* q = a.c.out + o;
+  if (!any_post(a.c.pf)) {
 #pragma unroll
-  for (int i = 0; i < S::R; ++i) {
-    const int k = t + i * T;
-    float2 X = __fmul2_rn(v[i], sg);
-    if (any_post(a.c.pf)) X = post_hook(X, k, M, a.c.pf);
-    sm[pidx(k)] = X;
+    for (int i = 0; i < S::R; ++i) __stcg(q + (long long)(t + i * T) * st, __fmul2_rn(v[i], sg));
+  } else {
+#pragma unroll
+    for (int i = 0; i < S::R; ++i) {
+      const int k = t + i * T;
+      __stcg(q + (long long)k * st, post_hook(__fmul2_rn(v[i], sg), k, M, a.c.pf));
+    }
   }
-  __syncthreads();
-  for (int idx = threadIdx.x; idx < G * M; idx += BLOCK) {
-    const int gg = idx & (G - 1), n = idx / G;
-    const long long o = off[gg];
-    if (o >= 0) a.c.out[o + (long long)n * st] = smem[gg * GS + pidx(n)];
+}
+
+// Lines per block wanted (2, 4 or 8; FFTFREE_2D_LINES, default 4), before
+// the shared-memory cap.
+static int lines_wanted() {
+  static const int w = [] {
+    const char* e = std::getenv("FFTFREE_2D_LINES");
+    const int v = e ? std::atoi(e) : 4;
+    return (v == 2 || v == 8) ? v : 4;
+  }();
+  return w;
+}
+
+template <int LOGM, int LOGR, int WANT>
+static cudaError_t run_strided_w(const StridedLinesArgs& a, cudaStream_t st, uint64_t* launches) {
+  using S = Sched<LOGM, LOGR>;
+  if constexpr (S::T > 1024) {
+    return cudaErrorInvalidValue;
+  } else {
+    using L = LinesLaunch<S, WANT>;
+    const long long grid = (a.c.batch + L::G - 1) / L::G;
+    if (grid <= 0) return cudaSuccess;
+    if (grid > 0x7fffffffLL) return cudaErrorInvalidValue;
+    if (L::SMEM_BYTES > 48 * 1024) {
+      cudaError_t e = cudaFuncSetAttribute(k_fft_strided<S, WANT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                           (int)L::SMEM_BYTES);
+      if (e != cudaSuccess) return e;
+    }
+    Twiddles tw{twiddle_pyramid(0, st), twiddle_pass_tables(st)};
+    k_fft_strided<S, WANT><<<(unsigned)grid, L::BLOCK, L::SMEM_BYTES, st>>>(a, tw);
+    if (launches) ++*launches;
+    return cudaGetLastError();
   }
 }
 
 template <int LOGM, int LOGR>
 static cudaError_t run_strided(const StridedLinesArgs& a, cudaStream_t st, uint64_t* launches) {
-  using S = Sched<LOGM, LOGR>;
-  if constexpr (S::T > 1024) {
-    return cudaErrorInvalidValue;
-  } else {
-    using L = LinesLaunch<S>;
-    const long long grid = (a.c.batch + L::G - 1) / L::G;
-    if (grid <= 0) return cudaSuccess;
-    if (grid > 0x7fffffffLL) return cudaErrorInvalidValue;
-    if (L::SMEM_BYTES > 48 * 1024) {
-      cudaError_t e = cudaFuncSetAttribute(k_fft_strided<S>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                           (int)L::SMEM_BYTES);
-      if (e != cudaSuccess) return e;
-    }
-    Twiddles tw{twiddle_pyramid(0, st), twiddle_pass_tables(st)};
-    k_fft_strided<S><<<(unsigned)grid, L::BLOCK, L::SMEM_BYTES, st>>>(a, tw);
-    if (launches) ++*launches;
-    return cudaGetLastError();
+  switch (lines_wanted()) {
+    case 2: return run_strided_w<LOGM, LOGR, 2>(a, st, launches);
+    case 8: return run_strided_w<LOGM, LOGR, 8>(a, st, launches);
+    default: return run_strided_w<LOGM, LOGR, 4>(a, st, launches);
   }
 }
 
