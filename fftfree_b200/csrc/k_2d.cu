@@ -9,8 +9,14 @@
 // x % G as engine thread x / G, so consecutive threads load and store
 // consecutive lines -- adjacent addresses, whole 32-byte sectors for G >= 4
 // -- straight between HBM and registers; shared memory only carries the
-// engine's exchanges.  Lines longer than the single-pass engine
-// (cols > 2^13) take the transpose / multi-pass / transpose route.
+// engine's exchanges.  When G divides the row count (every block's lines in
+// one matrix) the lines move by TMA instead (k_fft_strided_tma: the block's
+// whole input in flight at once, measured 1.0-1.25x the load/store form);
+// FFTFREE_2D_TMA=0 keeps the load/store form.  Lines longer than the
+// single-pass engine (cols > 2^13) take the transpose / multi-pass /
+// transpose route.
+#include <cuda.h>  // CUtensorMap and the encoder's types (the encoder is reached through the runtime)
+
 #include <cstdlib>
 
 #include "fft_launch.cuh"
@@ -83,15 +89,18 @@ __global__ void __launch_bounds__(LinesLaunch<S, WANT>::BLOCK) k_fft_strided(Str
   }
 }
 
-// Lines per block wanted (2, 4 or 8; FFTFREE_2D_LINES, default 4), before
-// the shared-memory cap.
-static int lines_wanted() {
-  static const int w = [] {
+// Lines per block wanted (2, 4 or 8; FFTFREE_2D_LINES), before the
+// shared-memory cap.  Default from B200 sweeps of the TMA kernel: 2 for
+// lines of 4096 points and more (two blocks per SM overlap load, compute
+// and store: 3.26 vs 2.89 TB/s at 4096), 4 below (2048: 4.10 vs 3.62).
+static int lines_wanted(int logm) {
+  static const int env = [] {
     const char* e = std::getenv("FFTFREE_2D_LINES");
-    const int v = e ? std::atoi(e) : 4;
-    return (v == 2 || v == 8) ? v : 4;
+    const int v = e ? std::atoi(e) : 0;
+    return (v == 2 || v == 4 || v == 8) ? v : 0;
   }();
-  return w;
+  if (env) return env;
+  return logm >= 12 ? 2 : 4;
 }
 
 template <int LOGM, int LOGR, int WANT>
@@ -116,9 +125,194 @@ static cudaError_t run_strided_w(const StridedLinesArgs& a, cudaStream_t st, uin
   }
 }
 
+// ------------------------------------------------------------------ TMA variant
+// The same transform with the G lines moved by the Tensor Memory Accelerator:
+// one thread issues boxes of G lines x BN elements (a 3-D tensor map over
+// rows x cols x batch, 8-byte elements) into a [n][line] staging tile, the
+// whole block's input in flight at once; the result leaves the same way
+// through TMA stores.  The engine's tiles reuse the staging space.
+__device__ unsigned int g_strided_tma_timeouts = 0;  // bounded mbarrier waits that gave up
+
+__device__ __forceinline__ uint32_t smem_addr(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ bool mbar_wait_parity(uint32_t bar, uint32_t parity, unsigned limit) {
+  for (unsigned it = 0; it < limit; ++it) {
+    uint32_t done;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(done)
+        : "r"(bar), "r"(parity)
+        : "memory");
+    if (done) return true;
+  }
+  return false;
+}
+
+template <class S, int WANT>
+__global__ void __launch_bounds__(LinesLaunch<S, WANT>::BLOCK)
+    k_fft_strided_tma(const __grid_constant__ CUtensorMap map_in, const __grid_constant__ CUtensorMap map_out,
+                      StridedLinesArgs a, Twiddles tw) {
+  using L = LinesLaunch<S, WANT>;
+  constexpr int G = L::G;
+  constexpr int T = S::T, M = S::M, GS = L::GS;
+  constexpr int BN = M < 256 ? M : 256;  // elements per box (box: G x BN)
+  constexpr unsigned kLimit = 1u << 22;
+  extern __shared__ __align__(128) float2 smem[];
+  float2* stage = smem;  // [M][G] while loading and storing
+  uint64_t* bar = reinterpret_cast<uint64_t*>(smem + G * GS);
+  const uint32_t bar_a = smem_addr(bar);
+  const int g = threadIdx.x & (G - 1);
+  const int t = threadIdx.x / G;
+  const long long l0 = (long long)blockIdx.x * G;
+  const int mat = (int)(l0 / a.rows), r0 = (int)(l0 % a.rows);  // G | rows: one matrix
+  if (threadIdx.x == 0) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(bar_a) : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar_a), "r"(G * M * 8) : "memory");
+#pragma unroll 1
+    for (int n0 = 0; n0 < M; n0 += BN)
+      asm volatile(
+          "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], "
+          "[%5];" ::"r"(smem_addr(stage + n0 * G)),
+          "l"(reinterpret_cast<uint64_t>(&map_in)), "r"(r0), "r"(n0), "r"(mat), "r"(bar_a)
+          : "memory");
+  }
+  const bool ok = __syncthreads_and(mbar_wait_parity(bar_a, 0, kLimit));
+  if (!ok) {
+    // give up: record it, wait (bounded) for the copies still in flight
+    if (threadIdx.x == 0) {
+      atomicAdd(&g_strided_tma_timeouts, 1u);
+      (void)mbar_wait_parity(bar_a, 0, kLimit);
+    }
+    return;
+  }
+  float2 v[S::R];
+  const float2 sg_in = make_float2(1.f, a.c.inverse ? -1.f : 1.f);  // inverse = conj . forward . conj
+  if (a.c.pre == 0) {
+#pragma unroll
+    for (int i = 0; i < S::R; ++i) v[i] = __fmul2_rn(stage[(t + i * T) * G + g], sg_in);
+  } else {
+    const auto at = [stage, g](int n) { return stage[n * G + g]; };
+#pragma unroll
+    for (int i = 0; i < S::R; ++i) v[i] = __fmul2_rn(c2c_pre_elem(a.c, at, t + i * T), sg_in);
+  }
+  __syncthreads();
+  fft_engine<S, LaneBlockSync>(v, t, smem + g * GS, tw);
+  __syncthreads();
+  const float sc = a.c.inverse ? 1.0f / (float)M : 1.0f;
+  const float2 sg = make_float2(sc, a.c.inverse ? -sc : sc);
+#pragma unroll
+  for (int i = 0; i < S::R; ++i) {
+    const int k = t + i * T;
+    float2 X = __fmul2_rn(v[i], sg);
+    if (any_post(a.c.pf)) X = post_hook(X, k, M, a.c.pf);
+    stage[k * G + g] = X;
+  }
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");  // generic writes -> async proxy
+  __syncthreads();
+  if (threadIdx.x == 0) {
+#pragma unroll 1
+    for (int n0 = 0; n0 < M; n0 += BN)
+      asm volatile("cp.async.bulk.tensor.3d.global.shared::cta.tile.bulk_group [%0, {%1, %2, %3}], [%4];" ::"l"(
+                       reinterpret_cast<uint64_t>(&map_out)),
+                   "r"(r0), "r"(n0), "r"(mat), "r"(smem_addr(stage + n0 * G))
+                   : "memory");
+    asm volatile("cp.async.bulk.commit_group;" ::: "memory");
+    asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory");  // staging tile read out before exit
+  }
+}
+
+using EncodeTiledFn = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                                   const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
+                                   CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+static EncodeTiledFn encode_tiled() {
+  static const EncodeTiledFn fn = [] {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q{};
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) != cudaSuccess ||
+        q != cudaDriverEntryPointSuccess) {
+      cudaGetLastError();
+      return (EncodeTiledFn) nullptr;
+    }
+    return reinterpret_cast<EncodeTiledFn>(p);
+  }();
+  return fn;
+}
+
+// rows x cols x batch matrices of 8-byte elements, box G x bn x 1
+static bool make_lines_map(CUtensorMap* m, const void* base, long long rows, long long cols, long long batch, int g,
+                           int bn) {
+  const EncodeTiledFn enc = encode_tiled();
+  if (!enc) return false;
+  const cuuint64_t dims[3] = {(cuuint64_t)rows, (cuuint64_t)cols, (cuuint64_t)batch};
+  const cuuint64_t strides[2] = {(cuuint64_t)rows * 8, (cuuint64_t)(rows * cols) * 8};
+  const cuuint32_t box[3] = {(cuuint32_t)g, (cuuint32_t)bn, 1};
+  const cuuint32_t es[3] = {1, 1, 1};
+  return enc(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 3, const_cast<void*>(base), dims, strides, box, es,
+             CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+             CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
+static bool tma_wanted() {
+  static const bool on = [] {
+    const char* e = std::getenv("FFTFREE_2D_TMA");
+    return !(e && e[0] == '0');
+  }();
+  return on;
+}
+
+// TMA path when the lines of a block share one matrix (G | rows), the
+// strides are 16-byte multiples and both bases 16-byte aligned; returns
+// cudaErrorNotSupported to let the caller take the LSU kernel.
+template <int LOGM, int LOGR, int WANT>
+static cudaError_t run_strided_tma(const StridedLinesArgs& a, cudaStream_t st, uint64_t* launches) {
+  using S = Sched<LOGM, LOGR>;
+  if constexpr (S::T > 1024) {
+    return cudaErrorNotSupported;
+  } else {
+    using L = LinesLaunch<S, WANT>;
+    constexpr int G = L::G;
+    constexpr int BN = S::M < 256 ? S::M : 256;
+    if (!tma_wanted() || G < 2 || a.rows % G != 0 || (reinterpret_cast<uintptr_t>(a.c.in) & 15) ||
+        (reinterpret_cast<uintptr_t>(a.c.out) & 15) || a.rows > 0x7fffffffLL)
+      return cudaErrorNotSupported;
+    const long long batch = a.c.batch / a.rows;
+    if (batch * a.rows != a.c.batch || batch > 0x7fffffffLL) return cudaErrorNotSupported;
+    CUtensorMap mi, mo;
+    if (!make_lines_map(&mi, a.c.in, a.rows, S::M, batch, G, BN) ||
+        !make_lines_map(&mo, a.c.out, a.rows, S::M, batch, G, BN))
+      return cudaErrorNotSupported;
+    const size_t smem = L::SMEM_BYTES + 16;
+    if (smem > 48 * 1024) {
+      cudaError_t e = cudaFuncSetAttribute(k_fft_strided_tma<S, WANT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                           (int)smem);
+      if (e != cudaSuccess) return e;
+    }
+    const long long grid = a.c.batch / G;
+    if (grid > 0x7fffffffLL) return cudaErrorNotSupported;
+    Twiddles tw{twiddle_pyramid(0, st), twiddle_pass_tables(st)};
+    k_fft_strided_tma<S, WANT><<<(unsigned)grid, L::BLOCK, smem, st>>>(mi, mo, a, tw);
+    if (launches) ++*launches;
+    return cudaGetLastError();
+  }
+}
+
 template <int LOGM, int LOGR>
 static cudaError_t run_strided(const StridedLinesArgs& a, cudaStream_t st, uint64_t* launches) {
-  switch (lines_wanted()) {
+  if (a.c.batch > 0) {
+    cudaError_t e;
+    switch (lines_wanted(LOGM)) {
+      case 2: e = run_strided_tma<LOGM, LOGR, 2>(a, st, launches); break;
+      case 8: e = run_strided_tma<LOGM, LOGR, 8>(a, st, launches); break;
+      default: e = run_strided_tma<LOGM, LOGR, 4>(a, st, launches); break;
+    }
+    if (e != cudaErrorNotSupported) return e;
+  }
+  switch (lines_wanted(LOGM)) {
     case 2: return run_strided_w<LOGM, LOGR, 2>(a, st, launches);
     case 8: return run_strided_w<LOGM, LOGR, 8>(a, st, launches);
     default: return run_strided_w<LOGM, LOGR, 4>(a, st, launches);
