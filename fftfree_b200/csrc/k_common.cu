@@ -113,6 +113,88 @@ cudaError_t launch_gl_project(const float* mag, const float* tr, const float* ti
   return cudaGetLastError();
 }
 
+// ------------------------------------------------------------------ minimum phase
+// fft_cffi.cpp:2104-2160 (phase_infer_execute, mode 1).  Log-amplitude
+// spectrum: frame f, point k of N: log(max(eps, |X|)) with the half
+// spectrum mirrored (points N-k from k, k < N/2), imaginary parts 0.
+__global__ void k_minphase_log(const float* __restrict__ mag, float2* __restrict__ spec, long long frames, int N,
+                               int bins, int half) {
+  const long long total = frames * (long long)N;
+  const float eps = 1e-20f;
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < total;
+       i += (long long)gridDim.x * blockDim.x) {
+    const long long f = i / N;
+    const int k = (int)(i - f * N);
+    int src = k;
+    if (half) {
+      // k <= N/2 from bin k; N-k (0 < k < N/2) mirrors bin k
+      if (k > N / 2) src = N - k;
+    }
+    const float m = (src < bins) ? __ldg(mag + f * bins + src) : 0.f;
+    spec[i] = make_float2(logf(fmaxf(eps, m)), 0.f);
+  }
+}
+
+// Causal shaping of the real cepstrum: points 1 .. (N+1)/2 - 1 doubled,
+// N/2 + 1 .. N-1 cleared (point 0 and, for even N, N/2 kept).
+__global__ void k_minphase_fold(float2* __restrict__ cep, long long frames, int N) {
+  const long long total = frames * (long long)N;
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < total;
+       i += (long long)gridDim.x * blockDim.x) {
+    const int n = (int)(i % N);
+    if (n >= 1 && n < (N + 1) / 2) {
+      const float2 c = cep[i];
+      cep[i] = make_float2(2.0f * c.x, 2.0f * c.y);
+    } else if (n >= N / 2 + 1) {
+      cep[i] = make_float2(0.f, 0.f);
+    }
+  }
+}
+
+// Minimum-phase spectrum from the complex log spectrum L: exp(Re L) e^{i Im L},
+// bins 0 .. bins-1 of every frame into planar re / im.
+__global__ void k_minphase_exp(const float2* __restrict__ lg, float* __restrict__ re, float* __restrict__ im,
+                               long long frames, int N, int bins) {
+  const long long total = frames * (long long)bins;
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < total;
+       i += (long long)gridDim.x * blockDim.x) {
+    const long long f = i / bins;
+    const int k = (int)(i - f * bins);
+    const float2 L = lg[f * N + k];
+    const float a = expf(L.x);
+    float s, c;
+    sincosf(L.y, &s, &c);
+    re[i] = a * c;
+    im[i] = a * s;
+  }
+}
+
+static unsigned elem_blocks(long long n) {
+  long long b = (n + 255) / 256;
+  if (b > 148 * 32) b = 148 * 32;
+  return (unsigned)(b > 0 ? b : 1);
+}
+
+cudaError_t launch_minphase_log(const float* mag, float2* spec, long long frames, int N, int bins, int half,
+                                cudaStream_t s) {
+  if (frames <= 0 || N <= 0) return cudaSuccess;
+  k_minphase_log<<<elem_blocks(frames * N), 256, 0, s>>>(mag, spec, frames, N, bins, half);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_minphase_fold(float2* cep, long long frames, int N, cudaStream_t s) {
+  if (frames <= 0 || N <= 0) return cudaSuccess;
+  k_minphase_fold<<<elem_blocks(frames * N), 256, 0, s>>>(cep, frames, N);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_minphase_exp(const float2* lg, float* re, float* im, long long frames, int N, int bins,
+                                cudaStream_t s) {
+  if (frames <= 0 || bins <= 0) return cudaSuccess;
+  k_minphase_exp<<<elem_blocks(frames * bins), 256, 0, s>>>(lg, re, im, frames, N, bins);
+  return cudaGetLastError();
+}
+
 // ------------------------------------------------------------------ twiddles
 namespace {
 struct Pyramid {

@@ -135,6 +135,14 @@ cudaError_t launch_ola(const OlaArgs& a, cudaStream_t s, uint64_t* launches);
 // DC and, for even N, Nyquist imaginary parts cleared).
 cudaError_t launch_gl_project(const float* mag, const float* tr, const float* ti, float* re, float* im,
                               long long nbins, int bins, int half, int even_n, cudaStream_t s);
+// Minimum-phase reconstruction (phase inference mode 1): the log-amplitude
+// spectrum of every frame (half spectra mirrored), the causal fold of the
+// real cepstrum, and exp of the complex log spectrum into planar re / im.
+cudaError_t launch_minphase_log(const float* mag, float2* spec, long long frames, int N, int bins, int half,
+                                cudaStream_t s);
+cudaError_t launch_minphase_fold(float2* cep, long long frames, int N, cudaStream_t s);
+cudaError_t launch_minphase_exp(const float2* lg, float* re, float* im, long long frames, int N, int bins,
+                                cudaStream_t s);
 // Largest N (log2) of the magnitude-gradient kernel; 0 for unsupported.
 int max_mag_grad_log();
 cudaError_t launch_stft_mag_grad(const MagGradArgs& a, int logr, cudaStream_t s, uint64_t* launches);

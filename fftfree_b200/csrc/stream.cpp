@@ -270,6 +270,7 @@ struct PhaseCtx {
   int N = 0, hop = 0, half = 1, mode = 0, iterations = 0;
   void* fwd = nullptr;  // C2C forward context (mode 1)
   void* inv = nullptr;  // C2C inverse context (mode 1)
+  DevBuf d_mag, d_spec, d_cep, d_re, d_im;  // mode 1 working set on the device
 };
 
 FFT_CFFI_API void* phase_init(int N, int hop, int half_spectrum, int mode, int iterations) {
@@ -321,55 +322,47 @@ FFT_CFFI_API size_t phase_infer_execute(void* handle, const float* in_mag, size_
       return frames;
     }
     if (p->mode != 1) return 0;
-    // Minimum phase from the real cepstrum, all frames in two GPU batches.
+    // Minimum phase from the real cepstrum, every step on the device: the
+    // log-amplitude spectra, the inverse batch, the causal fold, the forward
+    // batch and exp(L) per bin.
     if (!p->inv) p->inv = fft_init_full(N, 1, 1, 1, 0, 0, nullptr, 0, 1, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 1);
     if (!p->fwd) p->fwd = fft_init_full(N, 1, 1, 0, 0, 0, nullptr, 0, 1, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 1);
     if (!p->inv || !p->fwd) return 0;
-    const float eps = 1e-20f;
-    std::vector<float> spec(frames * (size_t)N * 2, 0.0f);
-    for (size_t f = 0; f < frames; ++f) {
-      const size_t base = f * (size_t)bins;
-      float* s = spec.data() + f * (size_t)N * 2;
-      auto set_log = [&](int k, float m) {
-        s[2 * k] = std::log(std::max(eps, m));
-        s[2 * k + 1] = 0.0f;
-      };
-      set_log(0, in_mag[base]);
-      if (p->half) {
-        for (int k = 1; k < N / 2; ++k) {
-          set_log(k, in_mag[base + k]);
-          s[2 * (N - k)] = s[2 * k];
-          s[2 * (N - k) + 1] = s[2 * k + 1];
-        }
-        if ((N % 2) == 0) set_log(N / 2, in_mag[base + N / 2]);
-      } else {
-        for (int k = 1; k < N; ++k) set_log(k, in_mag[base + k]);
+    FftContext* ic = as_ctx(p->inv);
+    int prev = -1;
+    cudaGetDevice(&prev);
+    if (prev != ic->device) cudaSetDevice(ic->device);
+    struct Restore {
+      int dev;
+      ~Restore() {
+        if (dev >= 0) cudaSetDevice(dev);
       }
-    }
-    std::vector<float> tim(spec.size());
-    if (!fftfree_execute_c2c(p->inv, spec.data(), tim.data(), frames)) return 0;
-    for (size_t f = 0; f < frames; ++f) {
-      float* t = tim.data() + f * (size_t)N * 2;
-      for (int n = 1; n < (N + 1) / 2; ++n) {
-        t[2 * n] *= 2.0f;
-        t[2 * n + 1] *= 2.0f;
-      }
-      for (int n = N / 2 + 1; n < N; ++n) {
-        t[2 * n] = 0.0f;
-        t[2 * n + 1] = 0.0f;
-      }
-    }
-    if (!fftfree_execute_c2c(p->fwd, tim.data(), spec.data(), frames)) return 0;
-    for (size_t f = 0; f < frames; ++f) {
-      const size_t base = f * (size_t)bins;
-      const float* s = spec.data() + f * (size_t)N * 2;
-      for (int k = 0; k < bins; ++k) {
-        const float a = std::exp(s[2 * k]);
-        const float ph = s[2 * k + 1];
-        out_real[base + k] = a * std::cos(ph);
-        out_imag[base + k] = a * std::sin(ph);
-      }
-    }
+    } restore{prev != ic->device ? prev : -1};
+    auto ok = [](cudaError_t e) {
+      if (e != cudaSuccess) throw std::runtime_error("cuda");
+    };
+    cudaStream_t st = ic->stream;
+    const size_t nb = frames * (size_t)bins, nc = frames * (size_t)N;
+    float* mag = static_cast<float*>(p->d_mag.get(nb * sizeof(float)));
+    float2* spec = static_cast<float2*>(p->d_spec.get(nc * sizeof(float2)));
+    float2* cep = static_cast<float2*>(p->d_cep.get(nc * sizeof(float2)));
+    float* re = static_cast<float*>(p->d_re.get(nb * sizeof(float)));
+    float* im = static_cast<float*>(p->d_im.get(nb * sizeof(float)));
+    ok(cudaMemcpyAsync(mag, in_mag, nb * sizeof(float), cudaMemcpyDefault, st));
+    ok(launch_minphase_log(mag, spec, (long long)frames, N, bins, p->half ? 1 : 0, st));
+    ok(cudaStreamSynchronize(st));
+    if (!fftfree_execute_c2c(p->inv, reinterpret_cast<const float*>(spec), reinterpret_cast<float*>(cep), frames))
+      return 0;
+    ok(cudaStreamSynchronize(ic->stream));
+    ok(launch_minphase_fold(cep, (long long)frames, N, st));
+    ok(cudaStreamSynchronize(st));
+    if (!fftfree_execute_c2c(p->fwd, reinterpret_cast<const float*>(cep), reinterpret_cast<float*>(spec), frames))
+      return 0;
+    ok(cudaStreamSynchronize(as_ctx(p->fwd)->stream));
+    ok(launch_minphase_exp(spec, re, im, (long long)frames, N, bins, st));
+    ok(cudaMemcpyAsync(out_real, re, nb * sizeof(float), cudaMemcpyDefault, st));
+    ok(cudaMemcpyAsync(out_imag, im, nb * sizeof(float), cudaMemcpyDefault, st));
+    ok(cudaStreamSynchronize(st));
     return frames;
   } catch (...) {
     return 0;
