@@ -51,13 +51,20 @@ struct FftContext {
   std::vector<float> analysis_win, synthesis_win;
   bool windows_enabled = false;
   int apply_ola = 0;
-  // streaming state (fft_cffi.cpp:72-78)
-  std::vector<float> streaming_buffer;
-  size_t streaming_offset = 0;
-  std::vector<float> streaming_inverse_queue;
-  size_t streaming_inverse_offset = 0;
-  std::vector<float> streaming_inverse_accum;
-  std::vector<float> streaming_inverse_norm;
+  // streaming state (fft_cffi.cpp:72-78), resident on the device:
+  //  * the pushed samples not yet consumed are [s_off, s_end) of d_stream
+  //    (d_stream2: the target of a compaction when it fills up);
+  //  * the inverse side's overlap-add carry (acc_len = 0 or N) and COLA norm
+  //    (nrm_len = 0 or N), double-buffered;
+  //  * emitted samples waiting for the caller are [q_off, q_end) of d_queue.
+  DevBuf d_stream, d_stream2;
+  size_t s_off = 0, s_end = 0;
+  DevBuf d_acc, d_acc2, d_nrm, d_nrm2, d_ifr, d_sweight;
+  size_t acc_len = 0, nrm_len = 0;
+  int sweight_n = 0;
+  DevBuf d_queue, d_queue2;
+  size_t q_off = 0, q_end = 0;
+  DevBuf d_sre, d_sim, d_smg;  // push_pcm outputs the caller leaves NULL
 
   // --- device state ---
   int device = 0;

@@ -113,6 +113,40 @@ cudaError_t launch_gl_project(const float* mag, const float* tr, const float* ti
   return cudaGetLastError();
 }
 
+// ------------------------------------------------------------------ streaming ISTFT
+__global__ void k_stream_ola(StreamOlaArgs a) {
+  const long long total = a.count + (a.keep_carry ? a.N : 0);
+  for (long long j = (long long)blockIdx.x * blockDim.x + threadIdx.x; j < total;
+       j += (long long)gridDim.x * blockDim.x) {
+    float acc = (j < a.N) ? a.carry[j] : 0.f;
+    float nrm = (a.use_norm && j < a.N) ? a.carry_nrm[j] : 0.f;
+    long long f0 = (j >= a.N) ? (j - a.N) / a.E + 1 : 0;
+    long long f1 = j / a.E;
+    if (f1 > a.F - 1) f1 = a.F - 1;
+    for (long long f = f0; f <= f1; ++f) {
+      const int i = (int)(j - f * a.E);
+      acc += __ldg(a.frames + f * a.N + i);
+      if (a.use_norm) nrm += a.weight ? __ldg(a.weight + i) : 1.0f;
+    }
+    if (j < a.count) {
+      if (a.use_norm && fabsf(nrm) > 1e-12f) acc /= nrm;
+      a.out[j] = acc;
+    } else {
+      a.new_carry[j - a.count] = acc;
+      if (a.use_norm) a.new_nrm[j - a.count] = nrm;
+    }
+  }
+}
+
+cudaError_t launch_stream_ola(const StreamOlaArgs& a, cudaStream_t s) {
+  const long long total = a.count + (a.keep_carry ? a.N : 0);
+  if (total <= 0) return cudaSuccess;
+  long long blocks = (total + 255) / 256;
+  if (blocks > 148 * 32) blocks = 148 * 32;
+  k_stream_ola<<<(unsigned)blocks, 256, 0, s>>>(a);
+  return cudaGetLastError();
+}
+
 // ------------------------------------------------------------------ minimum phase
 // fft_cffi.cpp:2104-2160 (phase_infer_execute, mode 1).  Log-amplitude
 // spectrum: frame f, point k of N: log(max(eps, |X|)) with the half

@@ -135,6 +135,28 @@ cudaError_t launch_ola(const OlaArgs& a, cudaStream_t s, uint64_t* launches);
 // DC and, for even N, Nyquist imaginary parts cleared).
 cudaError_t launch_gl_project(const float* mag, const float* tr, const float* ti, float* re, float* im,
                               long long nbins, int bins, int half, int even_n, cudaStream_t s);
+// Streaming ISTFT step (fft_cffi.cpp:1597-1742): F inverse frames of N
+// samples overlap-added at spacing E = min(hop, N) onto the carried
+// accumulator; samples 0 .. count-1 of the sum leave (divided by the summed
+// COLA weights when `use_norm` and that sum exceeds 1e-12 in magnitude),
+// samples count .. count+N-1 become the next carry (`keep_carry`; else the
+// carry is cleared).  Sums run carry first, then frames in order, as the
+// reference's frame-by-frame accumulation does.
+struct StreamOlaArgs {
+  const float* frames;     // F x N
+  long long F;
+  int N, E;
+  const float* carry;      // N
+  const float* carry_nrm;  // N (use_norm)
+  const float* weight;     // N or nullptr (1)
+  int use_norm;
+  long long count;
+  float* out;              // count samples
+  int keep_carry;
+  float* new_carry;        // N
+  float* new_nrm;          // N (use_norm)
+};
+cudaError_t launch_stream_ola(const StreamOlaArgs& a, cudaStream_t s);
 // Minimum-phase reconstruction (phase inference mode 1): the log-amplitude
 // spectrum of every frame (half spectra mirrored), the causal fold of the
 // real cepstrum, and exp of the complex log spectrum into planar re / im.

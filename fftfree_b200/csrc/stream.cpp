@@ -31,10 +31,7 @@ bool verbose() {
 int stream_window(const FftContext* c) { return c->window > 0 ? c->window : c->N; }
 int stream_hop(const FftContext* c) { return c->hop > 0 ? c->hop : stream_window(c); }
 
-size_t stream_backlog(const FftContext* c) {
-  if (c->streaming_offset >= c->streaming_buffer.size()) return 0;
-  return c->streaming_buffer.size() - c->streaming_offset;
-}
+size_t stream_backlog(const FftContext* c) { return c->s_end > c->s_off ? c->s_end - c->s_off : 0; }
 
 size_t stream_available_frames(const FftContext* c) {
   const size_t backlog = stream_backlog(c);
@@ -48,54 +45,89 @@ size_t stream_bins(const FftContext* c) {
   return c->half_spectrum ? n / 2 + 1 : n;
 }
 
-void stream_compact(FftContext* c) {
-  if (c->streaming_offset == 0) return;
-  if (c->streaming_offset >= c->streaming_buffer.size()) {
-    c->streaming_buffer.clear();
-    c->streaming_offset = 0;
-    return;
+void check(cudaError_t e) {
+  if (e != cudaSuccess) throw std::runtime_error("cuda");
+}
+
+bool on_device(const void* p) {
+  cudaPointerAttributes at{};
+  if (cudaPointerGetAttributes(&at, p) != cudaSuccess) {
+    cudaGetLastError();
+    return false;
   }
-  c->streaming_buffer.erase(c->streaming_buffer.begin(),
-                            c->streaming_buffer.begin() + (std::ptrdiff_t)c->streaming_offset);
-  c->streaming_offset = 0;
+  return at.type == cudaMemoryTypeDevice || at.type == cudaMemoryTypeManaged;
 }
 
-size_t stream_inverse_pending(const FftContext* c) {
-  if (c->streaming_inverse_queue.empty()) return 0;
-  if (c->streaming_inverse_offset >= c->streaming_inverse_queue.size()) return 0;
-  return c->streaming_inverse_queue.size() - c->streaming_inverse_offset;
+// Room for `extra` more samples after [s_off, s_end): the backlog moves to
+// the front of a (possibly larger) second buffer when the first is full.
+float* stream_reserve(FftContext* c, size_t extra) {
+  const size_t backlog = stream_backlog(c);
+  const size_t cap = c->d_stream.cap / sizeof(float);
+  if (c->d_stream.p && c->s_end + extra <= cap) return static_cast<float*>(c->d_stream.p);
+  const size_t want = std::max<size_t>(2 * (backlog + extra), 1 << 16);
+  float* dst = static_cast<float*>(c->d_stream2.get(want * sizeof(float)));
+  if (backlog)
+    check(cudaMemcpyAsync(dst, static_cast<float*>(c->d_stream.p) + c->s_off, backlog * sizeof(float),
+                          cudaMemcpyDeviceToDevice, c->stream));
+  std::swap(c->d_stream.p, c->d_stream2.p);
+  std::swap(c->d_stream.cap, c->d_stream2.cap);
+  c->s_off = 0;
+  c->s_end = backlog;
+  return dst;
 }
 
-void stream_inverse_compact(FftContext* c) {
-  if (c->streaming_inverse_offset == 0) return;
-  if (c->streaming_inverse_offset >= c->streaming_inverse_queue.size()) {
-    c->streaming_inverse_queue.clear();
-    c->streaming_inverse_offset = 0;
-    return;
-  }
-  c->streaming_inverse_queue.erase(
-      c->streaming_inverse_queue.begin(),
-      c->streaming_inverse_queue.begin() + (std::ptrdiff_t)c->streaming_inverse_offset);
-  c->streaming_inverse_offset = 0;
+size_t queue_pending(const FftContext* c) { return c->q_end > c->q_off ? c->q_end - c->q_off : 0; }
+
+// Room for `extra` more emitted samples at the queue's tail.
+float* queue_reserve(FftContext* c, size_t extra) {
+  const size_t pending = queue_pending(c);
+  const size_t cap = c->d_queue.cap / sizeof(float);
+  if (c->d_queue.p && c->q_end + extra <= cap) return static_cast<float*>(c->d_queue.p);
+  const size_t want = std::max<size_t>(2 * (pending + extra), 1 << 14);
+  float* dst = static_cast<float*>(c->d_queue2.get(want * sizeof(float)));
+  if (pending)
+    check(cudaMemcpyAsync(dst, static_cast<float*>(c->d_queue.p) + c->q_off, pending * sizeof(float),
+                          cudaMemcpyDeviceToDevice, c->stream));
+  std::swap(c->d_queue.p, c->d_queue2.p);
+  std::swap(c->d_queue.cap, c->d_queue2.cap);
+  c->q_off = 0;
+  c->q_end = pending;
+  return dst;
 }
 
-size_t stream_inverse_emit(FftContext* c, float* out_pcm, size_t max_samples) {
-  const size_t pending = stream_inverse_pending(c);
+// fft_cffi.cpp:1425-1447: up to max_samples (0: all) queued samples to out_pcm
+size_t queue_emit(FftContext* c, float* out_pcm, size_t max_samples) {
+  const size_t pending = queue_pending(c);
   if (pending == 0) return 0;
   size_t take = pending;
   if (max_samples != 0 && take > max_samples) take = max_samples;
   if (!out_pcm || take == 0) return 0;
-  std::copy_n(c->streaming_inverse_queue.data() + c->streaming_inverse_offset, take, out_pcm);
-  c->streaming_inverse_offset += take;
-  stream_inverse_compact(c);
+  check(cudaMemcpyAsync(out_pcm, static_cast<float*>(c->d_queue.p) + c->q_off, take * sizeof(float),
+                        cudaMemcpyDefault, c->stream));
+  check(cudaStreamSynchronize(c->stream));
+  c->q_off += take;
+  if (c->q_off >= c->q_end) c->q_off = c->q_end = 0;
   return take;
 }
 
-float cola_weight(const FftContext* c, size_t i) {
-  if (!c->windows_enabled) return 1.0f;
-  const float a = (i < c->analysis_win.size()) ? c->analysis_win[i] : 1.0f;
-  const float s = (i < c->synthesis_win.size()) ? c->synthesis_win[i] : 1.0f;
-  return a * s;
+// cola_window_weight (fft_cffi.cpp:210-226) on the device: analysis x
+// synthesis taps with windows enabled, else nullptr (weight 1)
+const float* stream_weight(FftContext* c) {
+  if (!c->windows_enabled) return nullptr;
+  const int n = std::max(c->N, 1);
+  if (c->sweight_n != n) {
+    std::vector<float> w(n);
+    for (int i = 0; i < n; ++i) {
+      const float a = (size_t)i < c->analysis_win.size() ? c->analysis_win[i] : 1.0f;
+      const float s = (size_t)i < c->synthesis_win.size() ? c->synthesis_win[i] : 1.0f;
+      w[i] = a * s;
+    }
+    float* d = static_cast<float*>(c->d_sweight.get(n * sizeof(float)));
+    check(cudaMemcpyAsync(d, w.data(), n * sizeof(float), cudaMemcpyHostToDevice, c->stream));
+    check(cudaStreamSynchronize(c->stream));
+    c->sweight_n = n;
+  }
+  return static_cast<const float*>(c->d_sweight.p);
 }
 
 }  // namespace
@@ -108,12 +140,9 @@ extern "C" {
 FFT_CFFI_API void fft_stream_reset(void* handle) {
   FftContext* c = as_ctx(handle);
   if (!c) return;
-  c->streaming_buffer.clear();
-  c->streaming_offset = 0;
-  c->streaming_inverse_queue.clear();
-  c->streaming_inverse_offset = 0;
-  c->streaming_inverse_accum.clear();
-  c->streaming_inverse_norm.clear();
+  c->s_off = c->s_end = 0;
+  c->q_off = c->q_end = 0;
+  c->acc_len = c->nrm_len = 0;
 }
 
 FFT_CFFI_API size_t fft_stream_pending_frames(void* handle) {
@@ -129,139 +158,153 @@ FFT_CFFI_API size_t fft_stream_backlog_samples(void* handle) {
 FFT_CFFI_API size_t fft_stream_pending_pcm(void* handle) {
   FftContext* c = as_ctx(handle);
   if (!c || !c->inverse) return 0;
-  return stream_inverse_pending(c);
+  return queue_pending(c);
 }
 
 FFT_CFFI_API size_t fft_stream_push_pcm(void* handle, const float* pcm, size_t samples,
                                         float* out_real, float* out_imag, float* out_mag,
                                         size_t max_frames, int flush_mode) {
-  // fft_cffi.cpp:1508-1595.  The reference prints a diagnostic line on every
-  // call; here that needs FFTFREE_VERBOSE.
+  // fft_cffi.cpp:1508-1595.  The backlog lives on the device: a push appends
+  // the new samples (one copy) and the frames run straight from the backlog
+  // -- the reference's host re-framing into a chunk gives the same samples
+  // (frame f of the chunk is backlog[fH, fH + W)).  The reference prints a
+  // diagnostic line on every call; here that needs FFTFREE_VERBOSE.
   (void)flush_mode;
   FftContext* c = as_ctx(handle);
   if (!c) {
     if (verbose()) std::fprintf(stderr, "[fft_stream_push_pcm] handle is NULL\n");
     return 0;
   }
-  if (samples > 0 && pcm) c->streaming_buffer.insert(c->streaming_buffer.end(), pcm, pcm + samples);
-  const int W = stream_window(c), H = stream_hop(c);
-  if (verbose())
-    std::fprintf(stderr, "[fft_stream_push_pcm] samples=%zu W=%d H=%d offset=%zu buf_size=%zu\n",
-                 samples, W, H, c->streaming_offset, c->streaming_buffer.size());
-  if (W <= 0 || H <= 0) return 0;
-  const size_t backlog = stream_backlog(c);
-  const size_t available = stream_available_frames(c);
-  if (available == 0) return 0;
-  size_t frames = available;
-  if (max_frames != 0 && frames > max_frames) frames = max_frames;
-  size_t pcm_len = (size_t)W + (frames - 1) * (size_t)H;
-  if (pcm_len > backlog) pcm_len = backlog;
-  std::vector<float> chunk(pcm_len, 0.0f);
-  for (size_t f = 0; f < frames; ++f) {
-    const size_t fs = f * (size_t)H;
-    const size_t src = c->streaming_offset + fs;
-    for (int wi = 0; wi < W; ++wi) {
-      const size_t ci = fs + (size_t)wi;
-      if (ci >= chunk.size()) break;
-      float v = 0.0f;
-      if (src + (size_t)wi < c->streaming_buffer.size()) v = c->streaming_buffer[src + (size_t)wi];
-      chunk[ci] = v;
+  try {
+    int prev = -1;
+    cudaGetDevice(&prev);
+    if (prev != c->device) cudaSetDevice(c->device);
+    struct Restore {
+      int dev;
+      ~Restore() {
+        if (dev >= 0) cudaSetDevice(dev);
+      }
+    } restore{prev != c->device ? prev : -1};
+    if (samples > 0 && pcm) {
+      float* buf = stream_reserve(c, samples);
+      check(cudaMemcpyAsync(buf + c->s_end, pcm, samples * sizeof(float), cudaMemcpyDefault, c->stream));
+      // the caller may reuse its buffer on return (the reference copies it)
+      if (!on_device(pcm)) check(cudaStreamSynchronize(c->stream));
+      c->s_end += samples;
     }
+    const int W = stream_window(c), H = stream_hop(c);
+    if (verbose())
+      std::fprintf(stderr, "[fft_stream_push_pcm] samples=%zu W=%d H=%d backlog=%zu\n", samples, W, H,
+                   stream_backlog(c));
+    if (W <= 0 || H <= 0) return 0;
+    const size_t backlog = stream_backlog(c);
+    const size_t available = stream_available_frames(c);
+    if (available == 0) return 0;
+    size_t frames = available;
+    if (max_frames != 0 && frames > max_frames) frames = max_frames;
+    size_t pcm_len = (size_t)W + (frames - 1) * (size_t)H;
+    if (pcm_len > backlog) pcm_len = backlog;
+    const size_t bins = stream_bins(c);
+    const size_t ob = frames * bins * sizeof(float);
+    float* rt = out_real ? out_real : static_cast<float*>(c->d_sre.get(ob));
+    float* it = out_imag ? out_imag : static_cast<float*>(c->d_sim.get(ob));
+    float* mt = out_mag ? out_mag : static_cast<float*>(c->d_smg.get(ob));
+    const float* src = static_cast<const float*>(c->d_stream.p) + c->s_off;
+    const size_t produced = fft_execute_batched(handle, src, pcm_len, rt, it, mt, 2, 0, frames);
+    if (produced == 0) return 0;
+    c->s_off += produced * (size_t)H;
+    if (c->s_off >= c->s_end) c->s_off = c->s_end = 0;
+    return produced;
+  } catch (...) {
+    return 0;
   }
-  const size_t bins = stream_bins(c);
-  std::vector<float> lr(out_real ? 0 : frames * bins), li(out_imag ? 0 : frames * bins),
-      lm(out_mag ? 0 : frames * bins);
-  float* rt = out_real ? out_real : lr.data();
-  float* it = out_imag ? out_imag : li.data();
-  float* mt = out_mag ? out_mag : lm.data();
-  const size_t produced = fft_execute_batched(handle, chunk.data(), pcm_len, rt, it, mt, 2, 0, frames);
-  if (produced == 0) return 0;
-  c->streaming_offset += produced * (size_t)H;
-  stream_compact(c);
-  return produced;
 }
 
 FFT_CFFI_API size_t fft_stream_push_spectrum(void* handle, const float* in_real,
                                              const float* in_imag, size_t frames, float* out_pcm,
                                              size_t max_samples, int flush_mode) {
-  // fft_cffi.cpp:1597-1742
+  // fft_cffi.cpp:1597-1742 with the accumulator, the COLA norm and the queue
+  // of emitted samples on the device: one inverse batch and one overlap-add
+  // launch per push (k_stream_ola) in place of the per-frame host loop.
   FftContext* c = as_ctx(handle);
   if (!c || !c->inverse) return 0;
-  const size_t plan_n = (size_t)std::max(c->N, 1);
-  const size_t bins = stream_bins(c);
-  if (c->streaming_inverse_accum.size() != plan_n) c->streaming_inverse_accum.assign(plan_n, 0.0f);
-  const bool use_norm = (c->cola_mode == FFT_COLA_NORMALIZE);
-  if (use_norm) {
-    if (c->streaming_inverse_norm.size() != plan_n) c->streaming_inverse_norm.assign(plan_n, 0.0f);
-  } else {
-    c->streaming_inverse_norm.clear();
-  }
-  if (frames > 0) {
-    if (!in_real) return stream_inverse_emit(c, out_pcm, max_samples);
-    const size_t total_bins = frames * bins;
-    std::vector<float> tr(in_real, in_real + total_bins);
-    std::vector<float> ti;
-    const float* imag_ptr = nullptr;
-    if (in_imag) {
-      ti.assign(in_imag, in_imag + total_bins);
-      imag_ptr = ti.data();
+  try {
+    int prev = -1;
+    cudaGetDevice(&prev);
+    if (prev != c->device) cudaSetDevice(c->device);
+    struct Restore {
+      int dev;
+      ~Restore() {
+        if (dev >= 0) cudaSetDevice(dev);
+      }
+    } restore{prev != c->device ? prev : -1};
+    const size_t plan_n = (size_t)std::max(c->N, 1);
+    const int N = (int)plan_n;
+    const size_t nb = plan_n * sizeof(float);
+    if (c->acc_len != plan_n) {
+      check(cudaMemsetAsync(c->d_acc.get(nb), 0, nb, c->stream));
+      c->acc_len = plan_n;
     }
-    std::vector<float> frame_pcm(frames * plan_n, 0.0f);
-    // A NULL imaginary part fails the batch (as in the reference), which then
-    // only drains what is queued.
-    size_t produced = fft_execute_complex_batched(handle, tr.data(), imag_ptr, frames,
-                                                  frame_pcm.data(), 2, 0, frames);
-    if (produced == 0) return stream_inverse_emit(c, out_pcm, max_samples);
-    if (produced > frames) produced = frames;
-    const size_t hop = (size_t)std::max(stream_hop(c), 1);
-    for (size_t f = 0; f < produced; ++f) {
-      const float* fr = frame_pcm.data() + f * plan_n;
-      for (size_t i = 0; i < plan_n; ++i) {
-        c->streaming_inverse_accum[i] += fr[i];
-        if (use_norm) c->streaming_inverse_norm[i] += cola_weight(c, i);
+    const bool use_norm = (c->cola_mode == FFT_COLA_NORMALIZE);
+    if (use_norm) {
+      if (c->nrm_len != plan_n) {
+        check(cudaMemsetAsync(c->d_nrm.get(nb), 0, nb, c->stream));
+        c->nrm_len = plan_n;
       }
-      size_t emit = hop;
-      if (flush_mode == FFT_STREAM_FLUSH_FINAL && (f + 1 == produced)) emit = plan_n;
-      if (emit > plan_n) emit = plan_n;
-      for (size_t i = 0; i < emit; ++i) {
-        float s = c->streaming_inverse_accum[i];
-        if (use_norm) {
-          const float d = c->streaming_inverse_norm[i];
-          if (std::fabs(d) > 1e-12f) s /= d;
-        }
-        c->streaming_inverse_queue.push_back(s);
-      }
-      if (emit < plan_n) {
-        std::move(c->streaming_inverse_accum.begin() + emit, c->streaming_inverse_accum.end(),
-                  c->streaming_inverse_accum.begin());
-        std::fill(c->streaming_inverse_accum.end() - emit, c->streaming_inverse_accum.end(), 0.0f);
-        if (use_norm) {
-          std::move(c->streaming_inverse_norm.begin() + emit, c->streaming_inverse_norm.end(),
-                    c->streaming_inverse_norm.begin());
-          std::fill(c->streaming_inverse_norm.end() - emit, c->streaming_inverse_norm.end(), 0.0f);
-        }
-      } else {
-        std::fill(c->streaming_inverse_accum.begin(), c->streaming_inverse_accum.end(), 0.0f);
-        if (use_norm) std::fill(c->streaming_inverse_norm.begin(), c->streaming_inverse_norm.end(), 0.0f);
-      }
+    } else {
+      c->nrm_len = 0;
     }
-  }
-  if (flush_mode == FFT_STREAM_FLUSH_FINAL && frames == 0) {
-    if (!c->streaming_inverse_accum.empty()) {
-      const bool nl = !c->streaming_inverse_norm.empty();
-      for (size_t i = 0; i < c->streaming_inverse_accum.size(); ++i) {
-        float s = c->streaming_inverse_accum[i];
-        if (nl) {
-          const float d = c->streaming_inverse_norm[i];
-          if (std::fabs(d) > 1e-12f) s /= d;
-        }
-        c->streaming_inverse_queue.push_back(s);
-      }
-      std::fill(c->streaming_inverse_accum.begin(), c->streaming_inverse_accum.end(), 0.0f);
-      if (nl) std::fill(c->streaming_inverse_norm.begin(), c->streaming_inverse_norm.end(), 0.0f);
+    const bool final_flush = (flush_mode == FFT_STREAM_FLUSH_FINAL);
+    StreamOlaArgs o{};
+    o.N = N;
+    o.E = (int)std::min<size_t>((size_t)std::max(stream_hop(c), 1), plan_n);
+    o.carry = static_cast<const float*>(c->d_acc.p);
+    o.carry_nrm = use_norm ? static_cast<const float*>(c->d_nrm.p) : nullptr;
+    o.weight = use_norm ? stream_weight(c) : nullptr;
+    o.use_norm = use_norm ? 1 : 0;
+    o.keep_carry = final_flush ? 0 : 1;
+    bool run = false;
+    if (frames > 0) {
+      if (!in_real) return queue_emit(c, out_pcm, max_samples);
+      // A NULL imaginary part fails the batch (as in the reference), which
+      // then only drains what is queued.
+      float* fr = static_cast<float*>(c->d_ifr.get(frames * plan_n * sizeof(float)));
+      size_t produced = fft_execute_complex_batched(handle, in_real, in_imag, frames, fr, 2, 0, frames);
+      if (produced == 0) return queue_emit(c, out_pcm, max_samples);
+      if (produced > frames) produced = frames;
+      o.frames = fr;
+      o.F = (long long)produced;
+      o.count = final_flush ? (long long)(produced - 1) * o.E + N : (long long)produced * o.E;
+      run = true;
+    } else if (final_flush) {
+      // FINAL with no frames: the whole carry leaves
+      o.frames = nullptr;
+      o.F = 0;
+      o.count = N;
+      run = true;
     }
+    if (run) {
+      float* q = queue_reserve(c, (size_t)o.count);  // may move the queue (q_end changes)
+      o.out = q + c->q_end;
+      o.new_carry = static_cast<float*>(c->d_acc2.get(nb));
+      o.new_nrm = use_norm ? static_cast<float*>(c->d_nrm2.get(nb)) : nullptr;
+      check(launch_stream_ola(o, c->stream));
+      if (!o.keep_carry) {
+        check(cudaMemsetAsync(o.new_carry, 0, nb, c->stream));
+        if (use_norm) check(cudaMemsetAsync(o.new_nrm, 0, nb, c->stream));
+      }
+      std::swap(c->d_acc.p, c->d_acc2.p);
+      std::swap(c->d_acc.cap, c->d_acc2.cap);
+      if (use_norm) {
+        std::swap(c->d_nrm.p, c->d_nrm2.p);
+        std::swap(c->d_nrm.cap, c->d_nrm2.cap);
+      }
+      c->q_end += (size_t)o.count;
+    }
+    return queue_emit(c, out_pcm, max_samples);
+  } catch (...) {
+    return 0;
   }
-  return stream_inverse_emit(c, out_pcm, max_samples);
 }
 
 // ------------------------------------------------------------------ phase inference

@@ -170,3 +170,59 @@ def test_phase_infer_matches_oracle(N, half):
         else:
             rre, rim = sg.phase_min(mag, frames, N, bool(half))
             assert_close(re + 1j * im, (rre + 1j * rim).ravel(), 10 * tol_for(N), "minimum phase")
+
+
+def test_stream_push_pcm_large_pushes_device_input_and_null_outputs():
+    """Pushes larger than the device backlog's first allocation (it grows and
+    compacts), a device-resident chunk, and a push with NULL outputs (the
+    frames are consumed, as in the reference)."""
+    N, W, H = 256, 256, 64
+    kw = ctx_kwargs(N, transform=1, half_spectrum=1, window=W, hop=H, apply_windows=1, analysis_kind=1)
+    ctx = api.FftContext.full_v2(**kw)
+    st = sg.StreamOracle(oracle_for(kw))
+    bins = N // 2 + 1
+    rng = np.random.default_rng(77)
+    L = api.lib()
+    for n_in, dev, mf, null_out in [(100_000, False, 0, False), (70_001, True, 500, False), (3, False, 0, True),
+                                    (150_000, False, 0, False), (0, False, 0, False)]:
+        x = rng.uniform(-1, 1, n_in).astype(np.float32)
+        src = torch.from_numpy(x).cuda() if dev else x
+        cap = (n_in + 1024) // H + 2
+        re = np.zeros(cap * bins, np.float32)
+        im = np.zeros_like(re)
+        mg = np.zeros_like(re)
+        if null_out:
+            n = L.fft_stream_push_pcm(ctx.handle, _fp(src) if n_in else None, n_in, None, None, None, mf, 0)
+        else:
+            n = L.fft_stream_push_pcm(ctx.handle, _fp(src) if n_in else None, n_in, _fp(re), _fp(im), _fp(mg), mf, 0)
+        rn, rre, rim, rmg = st.push_pcm(x, mf)
+        assert n == rn
+        assert L.fft_stream_backlog_samples(ctx.handle) == len(st.buffer)
+        if n and not null_out:
+            k = n * bins
+            assert_close(re[:k] + 1j * im[:k], (rre + 1j * rim).ravel(), tol_for(N), "stream spectrum")
+
+
+def test_stream_push_spectrum_long_queue():
+    """Many frames per push with the queue drained in small pieces: the
+    device queue grows while samples are pending."""
+    N, H = 128, 32
+    kw = ctx_kwargs(N, inverse=1, transform=2, half_spectrum=1, window=N, hop=H, apply_windows=1,
+                    analysis_kind=1, synthesis_kind=1, cola_mode=1)
+    ctx = api.FftContext.full_v2(**kw)
+    st = sg.StreamOracle(oracle_for(kw))
+    bins = N // 2 + 1
+    rng = np.random.default_rng(5)
+    L = api.lib()
+    got, ref = [], []
+    for frames, ms, fl in [(300, 1000, 0), (400, 3000, 0), (0, 0, 0), (250, 0, sg.FLUSH_FINAL), (0, 0, 0)]:
+        re = rng.standard_normal(max(frames, 1) * bins).astype(np.float32)
+        im = rng.standard_normal(max(frames, 1) * bins).astype(np.float32)
+        out = np.zeros(64000, np.float32)
+        n = L.fft_stream_push_spectrum(ctx.handle, _fp(re), _fp(im), frames, _fp(out), ms, fl)
+        r = st.push_spectrum(re, im, frames, ms, fl)
+        assert n == len(r)
+        assert L.fft_stream_pending_pcm(ctx.handle) == len(st.queue)
+        got.append(out[:n])
+        ref.append(r)
+    assert_close(np.concatenate(got), np.concatenate(ref), tol_for(N), "stream pcm")
