@@ -99,6 +99,10 @@ _SIGS = [
     ("fftfree_device_available", ctypes.c_int, []),
     ("fftfree_execute_complex_batched_noalloc", ctypes.c_size_t, [ctypes.c_void_p, c_float_p, c_float_p,
                                                                    ctypes.c_size_t, c_float_p, ctypes.c_size_t]),
+    ("ft_apply_complex_pipeline", ctypes.c_int, [ctypes.c_void_p] * 4 + [c_float_p, c_float_p, ctypes.c_int,
+                                                                          ctypes.c_int]),
+    ("ft_apply_polar_pipeline", ctypes.c_int, [ctypes.c_void_p] * 4 + [c_float_p, c_float_p, ctypes.c_int,
+                                                                        ctypes.c_int]),
     ("fftfree_execute_2d", ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, c_float_p, c_float_p, ctypes.c_size_t,
                                           ctypes.c_size_t, ctypes.c_size_t]),
     ("fftfree_stft_magnitude", ctypes.c_size_t, [ctypes.c_void_p, c_float_p, ctypes.c_size_t, ctypes.c_size_t,
@@ -327,6 +331,46 @@ class RaggedPlan:
             self.close()
         except Exception:
             pass
+
+
+class FtGridSpec(ctypes.Structure):
+    """struct ft_grid_spec (ft_tools_cffi.hpp:9-14)."""
+    _fields_ = [("time_origin", ctypes.c_double), ("freq_origin", ctypes.c_double),
+                ("time_step", ctypes.c_double), ("freq_step", ctypes.c_double)]
+
+
+class FtResamplePlan(ctypes.Structure):
+    """struct ft_resample_plan_c (ft_tools_cffi.hpp:16-22)."""
+    _fields_ = [("upsample_time", ctypes.c_int), ("upsample_freq", ctypes.c_int),
+                ("downsample_time", ctypes.c_int), ("downsample_freq", ctypes.c_int),
+                ("preserve_energy", ctypes.c_int)]
+
+
+class FtQuantizerConfig(ctypes.Structure):
+    """struct ft_quantizer_config (ft_tools_cffi.hpp:24-30)."""
+    _fields_ = [("enabled", ctypes.c_int), ("base_frequency", ctypes.c_float), ("magnitude_step", ctypes.c_float),
+                ("mix", ctypes.c_float), ("distance_decay", ctypes.c_float)]
+
+
+class FtContrastConfig(ctypes.Structure):
+    """struct ft_contrast_config (ft_tools_cffi.hpp:32-40)."""
+    _fields_ = [("enabled", ctypes.c_int), ("kernel_time", ctypes.c_int), ("kernel_freq", ctypes.c_int),
+                ("brightness", ctypes.c_float), ("contrast", ctypes.c_float), ("gamma", ctypes.c_float),
+                ("clamp_zero", ctypes.c_int)]
+
+
+def _byref(x):
+    return ctypes.byref(x) if x is not None else None
+
+
+def ft_apply_pipeline(a, b, time_bins: int, freq_bins: int, spec=None, plan=None, quant=None, contrast=None,
+                      polar: bool = False) -> int:
+    """ft_apply_complex_pipeline / ft_apply_polar_pipeline on planar float32
+    grids (time_bins rows of freq_bins; host arrays or CUDA tensors), in
+    place.  ``spec`` / ``plan`` / ``quant`` / ``contrast`` are the ctypes
+    structs above or None."""
+    fn = lib().ft_apply_polar_pipeline if polar else lib().ft_apply_complex_pipeline
+    return int(fn(_byref(spec), _byref(plan), _byref(quant), _byref(contrast), _fp(a), _fp(b), time_bins, freq_bins))
 
 
 def execute_2d(ctx_axis0: "FftContext", ctx_axis1: "FftContext", x, out, rows: int, cols: int,

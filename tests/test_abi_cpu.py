@@ -18,7 +18,9 @@ REPO = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 
 def _declared_symbols():
     names = set()
-    for h in ("fft_cffi.h", "fftfree_b200.h"):
+    for h in sorted(os.listdir(os.path.join(REPO, "include"))):
+        if not h.endswith(".h"):
+            continue
         src = open(os.path.join(REPO, "include", h)).read()
         for m in re.finditer(r"FFT_CFFI_API\s+[\w\s\*]+?\b(\w+)\s*\(", src):
             names.add(m.group(1))
@@ -45,7 +47,9 @@ def test_python_binding_covers_declarations():
 
 def _declared_arity():
     out = {}
-    for h in ("fft_cffi.h", "fftfree_b200.h"):
+    for h in sorted(os.listdir(os.path.join(REPO, "include"))):
+        if not h.endswith(".h"):
+            continue
         src = open(os.path.join(REPO, "include", h)).read()
         for m in re.finditer(r"FFT_CFFI_API\s+[\w\s\*]+?\b(\w+)\s*\(([^)]*)\)", src):
             params = m.group(2).strip()
