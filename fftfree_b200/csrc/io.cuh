@@ -25,6 +25,72 @@ __device__ __forceinline__ bool any_post(const PostFlags& pf) {
   return (pf.r2c_half | pf.polar | pf.reduce | pf.clear_imag) != 0;
 }
 
+// Phase and polar conversions of the hooks, written for throughput: the
+// polar epilogues spend most of their instructions here.
+//
+// atan2: octant reduction to a = min(|x|,|y|) / max(|x|,|y|) in [0, 1],
+// atan(a) = a P(a^2) with P of degree 7 fitted to atan on [0, 1] (weighted
+// least squares on Chebyshev nodes, coefficients rounded to float: 9.2e-8
+// rad), then pi/2 - r, pi - r and the sign of y as the octant says; C's
+// atan2 results for zero arguments.  Max error against FP64: 3.6e-7 rad.
+__device__ __forceinline__ float atan2_fast(float y, float x) {
+  const float ax = fabsf(x), ay = fabsf(y);
+  float mx = fmaxf(ax, ay), mn = fminf(ax, ay);
+  if (mx > 1e30f || mx < 1e-30f) {  // keep the fast division in its range
+    const float sc = (mx > 1e30f) ? 0x1p-64f : 0x1p64f;
+    mx *= sc;
+    mn *= sc;
+  }
+  const float a = __fdividef(mn, mx);
+  const float t = a * a;
+  float p = -0.004780322778970003f;
+  p = fmaf(p, t, 0.024556664749979973f);
+  p = fmaf(p, t, -0.05990409106016159f);
+  p = fmaf(p, t, 0.09942717105150223f);
+  p = fmaf(p, t, -0.14029406011104584f);
+  p = fmaf(p, t, 0.19971372187137604f);
+  p = fmaf(p, t, -0.3333209455013275f);
+  p = fmaf(p, t, 0.9999999403953552f);
+  float r = a * p;
+  if (ay > ax) r = 1.5707963705062866f - r;
+  if (signbit(x)) r = 3.1415927410125732f - r;
+  if (ax == 0.f && ay == 0.f) r = signbit(x) ? 3.1415927410125732f : 0.f;
+  return copysignf(r, y);
+}
+
+// sin and cos: Cody-Waite reduction by pi/2 split into three floats (with
+// FMA, exact to the float rounding of r for |x| <= 8192) to |r| <= pi/4,
+// sin(r) = r Q(r^2) and cos(r) = P(r^2) with Q of degree 3 and P of degree 4
+// fitted to sin(r)/r and cos(r) on [0, pi/4] (max 4e-9), the quadrant
+// swapping and negating them; larger |x| (and NaN) through sincosf.  Max
+// error against FP64: 8.7e-8.
+__device__ __forceinline__ void sincos_fast(float x, float* sn, float* cs) {
+  if (!(fabsf(x) <= 8192.f)) {
+    sincosf(x, sn, cs);
+    return;
+  }
+  const float k = rintf(x * 0.6366197466850281f);
+  float r = fmaf(-k, 1.5707963705062866f, x);
+  r = fmaf(-k, -4.371138828673793e-08f, r);
+  r = fmaf(-k, -1.7151245100058819e-15f, r);
+  const float t = r * r;
+  float q = -0.00019504022202454507f;
+  q = fmaf(q, t, 0.008332036435604095f);
+  q = fmaf(q, t, -0.16666650772094727f);
+  q = fmaf(q, t, 1.0f);
+  const float s0 = r * q;
+  float c = 2.4379929527640343e-05f;
+  c = fmaf(c, t, -0.0013886619126424193f);
+  c = fmaf(c, t, 0.04166661575436592f);
+  c = fmaf(c, t, -0.5f);
+  const float c0 = fmaf(c, t, 1.0f);
+  const int quad = (int)k & 3;
+  const float ss = (quad & 1) ? c0 : s0;
+  const float cc = (quad & 1) ? s0 : c0;
+  *sn = (quad & 2) ? -ss : ss;
+  *cs = ((quad + 1) & 2) ? -cc : cc;
+}
+
 __device__ __forceinline__ float2 post_hook(float2 X, int k, int N, const PostFlags& pf) {
   // eigen_fft.hpp:2544-2595.  Polar/reduce apply below `upper`; above it the
   // R2C half branch has already zeroed the value, and (0,0) is a fixed point
@@ -35,7 +101,7 @@ __device__ __forceinline__ float2 post_hook(float2 X, int k, int N, const PostFl
   }
   if (pf.polar) {
     const float m = cabs_fast(X.x, X.y);
-    const float ph = atan2f(X.y, X.x);
+    const float ph = atan2_fast(X.y, X.x);
     X = make_float2(m, ph);
   } else if (pf.reduce) {
     X = make_float2(cabs_fast(X.x, X.y), 0.f);
@@ -47,7 +113,7 @@ __device__ __forceinline__ float2 post_hook(float2 X, int k, int N, const PostFl
 
 __device__ __forceinline__ float2 polar_to_complex(float2 u) {
   float s, c;
-  sincosf(u.y, &s, &c);
+  sincos_fast(u.y, &s, &c);
   return make_float2(u.x * c, u.x * s);
 }
 
@@ -62,7 +128,7 @@ __device__ __forceinline__ float2 post_hook_m(float2 X, int k, int N, const Post
     if (k > (N >> 1)) X = make_float2(0.f, 0.f);
     else if (k == 0 || k == (N >> 1)) X.y = 0.f;
   }
-  if constexpr (MODE == 2) return make_float2(cabs_fast(X.x, X.y), atan2f(X.y, X.x));
+  if constexpr (MODE == 2) return make_float2(cabs_fast(X.x, X.y), atan2_fast(X.y, X.x));
   if constexpr (MODE == 1) return make_float2(cabs_fast(X.x, X.y), 0.f);
   if (pf.clear_imag) X.y = 0.f;
   return X;
@@ -241,7 +307,7 @@ struct StftIO {
           continue;
         }
         float mag;
-        if constexpr (MODE == 2) { mag = cabs_fast(X.x, X.y); X = make_float2(mag, atan2f(X.y, X.x)); }
+        if constexpr (MODE == 2) { mag = cabs_fast(X.x, X.y); X = make_float2(mag, atan2_fast(X.y, X.x)); }
         else if constexpr (MODE == 1) { mag = cabs_fast(X.x, X.y); X = make_float2(mag, 0.f); }
         else {
           if (a.pf.clear_imag) X.y = 0.f;
