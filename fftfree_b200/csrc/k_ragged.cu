@@ -12,7 +12,8 @@
 // of the 256-thread block (the single-pass engine and the STFT load/store
 // policy, so these items match fft_execute_batched bit for bit), or one
 // item of 2^13 .. 2^15 complex points, which the block transforms in three
-// phases through its own global scratch (columns, rows, untangle).  Blocks
+// phases through its own global scratch (columns, rows, untangle; one slot
+// of 2^15 points per block, rewritten in place).  Blocks
 // take tiles from an atomic counter until the list is exhausted.
 #include "fft_launch.cuh"
 
@@ -69,8 +70,16 @@ __device__ __forceinline__ void ragged_large(const RaggedArgs& a, int4 tile, flo
   const int item = tile.x;
   const float* x = a.pcm + __ldg(a.pcm_off + item);
   const long long oo = __ldg(a.out_off + item);
-  float2* scr_a = a.scratch + (long long)blockIdx.x * (2LL << kLargeMax);
-  float2* scr_b = scr_a + (1LL << kLargeMax);
+  // one slot of M points per block: phase A writes the columns' results in
+  // row order, phase B overwrites each group of 16 rows, in place, with their
+  // results in [k2][row] order (contiguous stores), phase C reads Z[k] at
+  // zidx(k).  (A slot per block of M points keeps all blocks' scratch,
+  // 444 x 256 KiB, inside the 126 MB L2.)
+  float2* scr_a = a.scratch + (long long)blockIdx.x * (1LL << kLargeMax);
+  const auto zidx = [](int k) -> long long {
+    const int k1 = k & (M1 - 1), k2 = k >> LM1;
+    return (long long)(k1 >> 4) * 16 * M2 + (long long)k2 * 16 + (k1 & 15);
+  };
   float2* tiles = smem;
   float2* stage = smem + 16 * rtile<SA>();
   // phase A: 16 columns at a time, 16 threads each (lanes walk n2)
@@ -108,9 +117,10 @@ __device__ __forceinline__ void ragged_large(const RaggedArgs& a, int4 tile, flo
 #pragma unroll
       for (int i = 0; i < SB::R; ++i) stage[(t + 16 * i) * 17 + j] = v[i];
       __syncthreads();
+      // rows r0 .. r0+15 are in registers: their region takes the results
       for (int flat = threadIdx.x; flat < 16 * M2; flat += kBlock) {
         const int k2 = flat >> 4, jj = flat & 15;
-        scr_b[(r0 + jj) + (long long)M1 * k2] = stage[k2 * 17 + jj];
+        scr_a[(long long)r0 * M2 + flat] = stage[k2 * 17 + jj];
       }
       __syncthreads();
     }
@@ -129,12 +139,12 @@ __device__ __forceinline__ void ragged_large(const RaggedArgs& a, int4 tile, flo
   const float2* w = tw.pyr + ((2u << LM) - 1u);  // level log2 N
   for (int k = threadIdx.x; k <= M; k += kBlock) {
     if (k == M) {
-      const float2 z0 = scr_b[0];
+      const float2 z0 = scr_a[zidx(0)];
       io.emit(re, im, mg, M, make_float2(z0.x - z0.y, 0.f), true, 1.0f, mag_is_re);
       continue;
     }
-    const float2 zk = scr_b[k];
-    const float2 zm = scr_b[(M - k) & (M - 1)];
+    const float2 zk = scr_a[zidx(k)];
+    const float2 zm = scr_a[zidx((M - k) & (M - 1))];
     const float2 E = make_float2(0.5f * (zk.x + zm.x), 0.5f * (zk.y - zm.y));
     const float2 D = make_float2(zk.x - zm.x, zk.y + zm.y);
     const float2 O = make_float2(0.5f * D.y, -0.5f * D.x);
@@ -202,7 +212,7 @@ cudaError_t launch_mode(const RaggedArgs& a, int grid, cudaStream_t st, uint64_t
 
 int ragged_max_log() { return kLargeMax + 1; }  // log2 N of the largest item
 bool ragged_large_log(int logm) { return logm >= kLargeMin && logm <= kLargeMax; }
-size_t ragged_scratch_per_block() { return (2ull << kLargeMax) * sizeof(float2); }
+size_t ragged_scratch_per_block() { return (1ull << kLargeMax) * sizeof(float2); }
 
 int ragged_candidates(int logm, int* lrs) {
   if (logm >= kLargeMin) return 0;
