@@ -448,6 +448,34 @@ def measure_legs(ff, torch, stream, reps: int = 10):
     legs["c2r_n4096_half_polar"] = timed(lambda: c.execute_complex_batched(re, im, BATCH, out),
                                          2 * BATCH * bins * 4 + BATCH * N_FFT * 4)
     c.close()
+    # config 1 exactly: one call on one signal of 65,536 samples (U[-1,1),
+    # seed 0) -> 253 frames x 513 bins; a synchronous call, so its latency is
+    # host wall-clock per call (device buffers, and host buffers with the
+    # copies inside)
+    import time
+    x1 = np.random.default_rng(0).uniform(-1, 1, 65536).astype(np.float32)
+    c1 = ff.FftContext.full(1024, 1, 1, 0, 2, 4, None, 1, 1024, 256, 1, 1, 0, 1, 1, 0, 0, 0, 1)
+    nb1 = 253 * 513
+    hre1, him1, hmg1 = (np.zeros(nb1, np.float32) for _ in range(3))
+    dx1 = torch.from_numpy(x1).cuda()
+    dre1, dim1, dmg1 = (torch.empty(nb1, device="cuda") for _ in range(3))
+
+    def latency_us(fn, n=300):
+        for _ in range(20):
+            fn()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for _ in range(n):
+            fn()
+        torch.cuda.synchronize()
+        return (time.perf_counter() - t0) / n * 1e6
+
+    us_dev = latency_us(lambda: c1.execute_batched(dx1, dre1, dim1, dmg1, pcm_len=65536, pad_mode=1))
+    us_host = latency_us(lambda: c1.execute_batched(x1, hre1, him1, hmg1, pad_mode=1))
+    legs["stft_config1_single_call"] = {
+        "frames": 253, "us_device_buffers": round(us_dev, 2), "us_host_buffers": round(us_host, 2),
+        "frames_per_s_host_buffers": round(253 / (us_host * 1e-6), 1)}
+    c1.close()
     # config-1 shape on a long signal: N=W=1024, H=256, half, magnitude
     L = 512 * 65536
     pcm1 = torch.rand(L, device="cuda", generator=g) * 2 - 1
