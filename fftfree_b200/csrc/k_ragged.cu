@@ -84,15 +84,22 @@ __device__ __forceinline__ void ragged_large(const RaggedArgs& a, int4 tile, flo
   float2* stage = smem + 16 * rtile<SA>();
   // phase A: 16 columns at a time, 16 threads each (lanes walk n2)
   {
+    const bool x8 = (reinterpret_cast<uintptr_t>(x) & 7) == 0;
     const int c = threadIdx.x & 15, t = threadIdx.x >> 4;
 #pragma unroll 1
     for (int c0 = 0; c0 < M2; c0 += 16) {
       const int n2 = c0 + c;
       float2 v[SA::R];
+      if (x8) {  // z[m] = (x[2m], x[2m+1]) as one 8-byte load
+        const float2* x2 = reinterpret_cast<const float2*>(x);
 #pragma unroll
-      for (int i = 0; i < SA::R; ++i) {
-        const long long m = (long long)(t + 16 * i) * M2 + n2;
-        v[i] = make_float2(__ldg(x + 2 * m), __ldg(x + 2 * m + 1));
+        for (int i = 0; i < SA::R; ++i) v[i] = __ldg(x2 + (long long)(t + 16 * i) * M2 + n2);
+      } else {
+#pragma unroll
+        for (int i = 0; i < SA::R; ++i) {
+          const long long m = (long long)(t + 16 * i) * M2 + n2;
+          v[i] = make_float2(__ldg(x + 2 * m), __ldg(x + 2 * m + 1));
+        }
       }
       fft_engine<SA, BlockSync>(v, t, tiles + c * rtile<SA>(), tw);
 #pragma unroll
