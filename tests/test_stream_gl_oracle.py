@@ -141,3 +141,33 @@ def test_phase_linear_advance():
     k = np.arange(N // 2 + 1)
     want = np.angle(np.exp(1j * 2 * np.pi * k * H / N * 3))
     np.testing.assert_allclose(np.angle(np.exp(1j * (ph[3] - want))), 0, atol=1e-5)
+
+
+def test_stream_spectrum_hop_beyond_frame():
+    """A hop longer than the frame: each frame emits all of its N samples
+    (the emit count is min(hop, N)), so the stream is the frames back to back."""
+    N, H = 32, 48
+    fwd = OracleContext(N=N, transform=1, half_spectrum=1, window=N, hop=N)
+    inv = OracleContext(N=N, inverse=1, transform=2, half_spectrum=1, window=N, hop=H)
+    rng = np.random.default_rng(6)
+    x = rng.uniform(-1, 1, 5 * N).astype(np.float32)
+    n, re, im, _ = fwd.execute_batched(x, pad_mode=2)
+    assert n == 5
+    st = sg.StreamOracle(inv)
+    y = st.push_spectrum(re, im, n)
+    assert len(y) == n * N
+    np.testing.assert_allclose(y, x, rtol=0, atol=2e-5)
+
+
+def test_griffin_lim_full_spectrum():
+    """Full (non-half) spectra: the iterations keep the target magnitudes and
+    leave the DC / Nyquist imaginary parts alone."""
+    N, H, frames = 32, 8, 12
+    fwd = OracleContext(N=N, transform=0, half_spectrum=0, window=N, hop=H, apply_windows=1, analysis_kind=1)
+    inv = OracleContext(N=N, inverse=1, transform=0, half_spectrum=0, window=N, hop=H)
+    t = np.arange((frames - 1) * H + N)
+    x = np.sin(0.3 * t).astype(np.float32)
+    n, _, _, mag = fwd.execute_batched(x, pad_mode=1, max_frames=frames)
+    ok, re, im = sg.griffin_lim(fwd, inv, mag, frames, H, False, 3)
+    assert ok == 1 and re.shape == (frames, N)
+    np.testing.assert_allclose(np.hypot(re, im), mag, rtol=1e-5, atol=1e-6)
