@@ -96,6 +96,7 @@ _SIGS = [
     ("fftfree_set_async", None, [ctypes.c_void_p, ctypes.c_int]),
     ("fftfree_ctx_launch_count", ctypes.c_ulonglong, [ctypes.c_void_p]),
     ("fftfree_ctx_schedule", ctypes.c_int, [ctypes.c_void_p, c_int_p, ctypes.c_int]),
+    ("fftfree_ctx_kernel", ctypes.c_int, [ctypes.c_void_p]),
     ("fftfree_device_available", ctypes.c_int, []),
     ("fftfree_execute_complex_batched_noalloc", ctypes.c_size_t, [ctypes.c_void_p, c_float_p, c_float_p,
                                                                    ctypes.c_size_t, c_float_p, ctypes.c_size_t]),
@@ -228,6 +229,10 @@ class FftContext:
         n = lib().fftfree_ctx_schedule(self.handle, buf, 32)
         return list(buf[:n])
 
+    def kernel(self) -> int:
+        """Executor code after the FFTFREE_DEFAULT_KERNEL override."""
+        return int(lib().fftfree_ctx_kernel(self.handle))
+
     def launch_count(self) -> int:
         return int(lib().fftfree_ctx_launch_count(self.handle))
 
@@ -317,6 +322,10 @@ class RaggedPlan:
 
     def execute(self, pcm, out_real, out_imag, out_mag) -> int:
         return int(lib().fftfree_ragged_execute(self.handle, _fp(pcm), _fp(out_real), _fp(out_imag), _fp(out_mag)))
+
+    def kernel(self) -> int:
+        """Executor code after the FFTFREE_DEFAULT_KERNEL override."""
+        return int(lib().fftfree_ctx_kernel(self.handle))
 
     def launch_count(self) -> int:
         return int(lib().fftfree_ragged_launch_count(self.handle))

@@ -1326,6 +1326,11 @@ FFT_CFFI_API unsigned long long fftfree_ctx_launch_count(void* handle) {
   return c ? (unsigned long long)c->launches : 0ull;
 }
 
+FFT_CFFI_API int fftfree_ctx_kernel(void* handle) {
+  FftContext* c = as_ctx(handle);
+  return c ? c->kernel : -1;
+}
+
 FFT_CFFI_API int fftfree_ctx_schedule(void* handle, int* radices, int max_passes) {
   FftContext* c = as_ctx(handle);
   if (!c || !radices || max_passes <= 0) return 0;

@@ -76,6 +76,11 @@ FFT_CFFI_API unsigned long long fftfree_ctx_launch_count(void* handle);
  * transform; returns the number of passes written (at most max_passes). */
 FFT_CFFI_API int fftfree_ctx_schedule(void* handle, int* radices, int max_passes);
 
+/* The context's executor code after the FFTFREE_DEFAULT_KERNEL override of
+ * fft_init / fft_init_ex (fft_cffi.cpp:126-159, 553-558): 0 auto
+ * (Cooley-Tukey), 1 Cooley-Tukey, 2 Stockham; -1 for a NULL handle. */
+FFT_CFFI_API int fftfree_ctx_kernel(void* handle);
+
 /* 1 when a CUDA device is usable by this library, else 0. */
 FFT_CFFI_API int fftfree_device_available(void);
 

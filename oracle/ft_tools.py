@@ -1,5 +1,6 @@
-"""ctypes wrapper over the reference's own grid tools built as a checker
-(oracle/_ref/libft_tools_ref.so, from ft_tools.hpp by `make -C oracle ref`).
+"""ctypes wrapper over the reference's own grid tools built as a checker: the
+ft_apply_*_pipeline entry points of ft_tools_cffi.cpp, compiled unchanged into
+oracle/_ref/libfftfree_ref.so by `make -C oracle ref REF=<reference tree>`.
 
 TEST INFRASTRUCTURE ONLY: loaded by tests/ and by the fixture generator under
 tests/golden/; never by the product.  The structs mirror ft_tools_cffi.hpp:9-40.
@@ -12,8 +13,7 @@ import os
 import numpy as np
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
-REF_LIB = os.path.join(_HERE, "_ref", "libft_tools_ref.so")
-_lib = None
+REF_LIB = os.path.join(_HERE, "_ref", "libfftfree_ref.so")
 
 
 class GridSpec(ctypes.Structure):
@@ -43,16 +43,8 @@ def available() -> bool:
 
 
 def lib():
-    global _lib
-    if _lib is None:
-        L = ctypes.CDLL(REF_LIB)
-        fp = ctypes.POINTER(ctypes.c_float)
-        for name in ("ref_ft_apply_complex_pipeline", "ref_ft_apply_polar_pipeline"):
-            f = getattr(L, name)
-            f.argtypes = [ctypes.c_void_p] * 4 + [fp, fp, ctypes.c_int, ctypes.c_int]
-            f.restype = ctypes.c_int
-        _lib = L
-    return _lib
+    from oracle import reflib
+    return reflib.lib()
 
 
 def _ref(x):
@@ -65,7 +57,7 @@ def apply(a: np.ndarray, b: np.ndarray, T: int, F: int, spec=None, plan=None, qu
     (ok, a_out, b_out)."""
     a = np.ascontiguousarray(a, np.float32).copy()
     b = np.ascontiguousarray(b, np.float32).copy()
-    fn = lib().ref_ft_apply_polar_pipeline if polar else lib().ref_ft_apply_complex_pipeline
+    fn = lib().ft_apply_polar_pipeline if polar else lib().ft_apply_complex_pipeline
     fp = ctypes.POINTER(ctypes.c_float)
     ok = fn(_ref(spec), _ref(plan), _ref(quant), _ref(contrast), a.ctypes.data_as(fp), b.ctypes.data_as(fp), T, F)
     return int(ok), a, b

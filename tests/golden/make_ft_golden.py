@@ -1,9 +1,9 @@
 """Generate tests/golden/ft_tools_cases.npz: inputs and outputs of the
-reference's own spectrogram-grid tools (ft_tools.hpp, built from the
-reference tree into oracle/_ref/ by `make -C oracle ref`) for the grid
+reference's own spectrogram-grid tools (ft_tools_cffi.cpp over ft_tools.hpp,
+built from the reference tree into oracle/_ref/ by `make -C oracle ref`) for the grid
 pipeline cases of tests/test_gpu_ft_tools.py.
 
-    make -C oracle ref && python tests/golden/make_ft_golden.py
+    make -C oracle ref REF=<reference tree> && python tests/golden/make_ft_golden.py
 """
 import os
 import sys

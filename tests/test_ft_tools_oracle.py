@@ -1,5 +1,5 @@
-"""The grid-pipeline checker (the reference's own ft_tools.hpp built into
-oracle/_ref/) reproduces the committed fixtures, and its shape rule (CPU
+"""The grid-pipeline checker (the reference's own ft_tools_cffi.cpp built
+into oracle/_ref/) reproduces the committed fixtures, and its shape rule (CPU
 only; skipped where the reference tree was not available to build it)."""
 import os
 
