@@ -757,6 +757,9 @@ FFT_CFFI_API void fft_free(void* handle) {
     c->d_frames.release();
     c->d_meta_tw.release();
     c->d_scratch.release();
+    c->d_t2d.release();
+    c->d_tma_timeouts.release();
+    if (c->h_tma_timeouts) cudaFreeHost(c->h_tma_timeouts);
     for (cudaStream_t st : {c->up_stream, c->down_stream})
       if (st) {
         cudaStreamSynchronize(st);
@@ -1041,6 +1044,14 @@ FFT_CFFI_API int fftfree_execute_2d(void* ctx_axis0, void* ctx_axis1, const floa
     }
     DeviceGuard g(c0->device);
     cudaStream_t s = c0->stream;
+    // an earlier asynchronous call whose TMA row pass gave up reports here
+    if (c0->h_tma_timeouts && *(volatile unsigned*)c0->h_tma_timeouts) {
+      FFB_CHECK(cudaStreamSynchronize(s));
+      *c0->h_tma_timeouts = 0;
+      FFB_CHECK(cudaMemsetAsync(c0->d_tma_timeouts.get(sizeof(unsigned)), 0, sizeof(unsigned), s));
+      if (verbose()) std::fprintf(stderr, "[fftfree_b200] an earlier 2-D call's row pass gave up waiting\n");
+      return 0;
+    }
     const size_t n = batch * rows * cols * 2;
     const bool in_host = !is_device_ptr(in);
     OutTarget o = stage_out(c0->d_out0, out, n);
@@ -1049,9 +1060,19 @@ FFT_CFFI_API int fftfree_execute_2d(void* ctx_axis0, void* ctx_axis1, const floa
     run_c2c_lines(c0, c2c_args(c0, d_in, o.dev, batch * cols), s);
     // axis 1: row r of matrix m is the line of `cols` points r + j * rows
     C2cArgs a1 = c2c_args(c1, o.dev, o.dev, batch * rows);
+    bool tma_check = false;
     if (ilog2(cols) <= max_strided_log()) {
       StridedLinesArgs sl{a1, (long long)rows};
+      sl.timeouts = static_cast<unsigned*>(c0->d_tma_timeouts.get(sizeof(unsigned)));
+      if (!c0->h_tma_timeouts) {
+        FFB_CHECK(cudaHostAlloc(reinterpret_cast<void**>(&c0->h_tma_timeouts), sizeof(unsigned),
+                                cudaHostAllocDefault));
+        *c0->h_tma_timeouts = 0;
+        FFB_CHECK(cudaMemsetAsync(sl.timeouts, 0, sizeof(unsigned), s));
+      }
       FFB_CHECK(launch_c2c_strided(sl, c1->logr_req, s, &c1->launches));
+      FFB_CHECK(cudaMemcpyAsync(c0->h_tma_timeouts, sl.timeouts, sizeof(unsigned), cudaMemcpyDeviceToHost, s));
+      tma_check = true;
     } else {
       // lines beyond one pass: transpose, multi-pass over contiguous rows,
       // transpose back (the reference's own route)
@@ -1067,6 +1088,14 @@ FFT_CFFI_API int fftfree_execute_2d(void* ctx_axis0, void* ctx_axis1, const floa
     }
     finish_out(c0, o);
     finish_call(c0, in_host || o.host);
+    if (tma_check && (in_host || o.host || !c0->async) && *c0->h_tma_timeouts) {
+      // the call synchronised, so its count is here: a block gave up
+      *c0->h_tma_timeouts = 0;
+      FFB_CHECK(cudaMemsetAsync(c0->d_tma_timeouts.get(sizeof(unsigned)), 0, sizeof(unsigned), s));
+      FFB_CHECK(cudaStreamSynchronize(s));
+      if (verbose()) std::fprintf(stderr, "[fftfree_b200] 2-D row pass: a bounded wait gave up\n");
+      return 0;
+    }
     return 1;
   } catch (...) {
     return 0;

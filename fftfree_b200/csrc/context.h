@@ -78,6 +78,11 @@ struct FftContext {
   DevBuf d_meta_tw;  // reference float twiddle table for the metadata path
   DevBuf d_scratch;  // multi-pass intermediate chunk
   DevBuf d_t2d;      // transposed matrices of a 2-D transform with long rows
+  // 2-D row pass through TMA: the device count of blocks whose bounded wait
+  // gave up (cumulative until a call reports it) and its pinned host copy,
+  // refreshed by every such call when its stream reaches the copy
+  DevBuf d_tma_timeouts;
+  unsigned* h_tma_timeouts = nullptr;
   // host-buffer pipeline (abi.cpp): upload / download streams and events
   cudaStream_t up_stream = nullptr, down_stream = nullptr;
   std::vector<cudaEvent_t> pipe_events;

@@ -131,7 +131,6 @@ static cudaError_t run_strided_w(const StridedLinesArgs& a, cudaStream_t st, uin
 // rows x cols x batch, 8-byte elements) into a [n][line] staging tile, the
 // whole block's input in flight at once; the result leaves the same way
 // through TMA stores.  The engine's tiles reuse the staging space.
-__device__ unsigned int g_strided_tma_timeouts = 0;  // bounded mbarrier waits that gave up
 
 __device__ __forceinline__ uint32_t smem_addr(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
 
@@ -151,12 +150,12 @@ __device__ __forceinline__ bool mbar_wait_parity(uint32_t bar, uint32_t parity, 
 template <class S, int WANT>
 __global__ void __launch_bounds__(LinesLaunch<S, WANT>::BLOCK)
     k_fft_strided_tma(const __grid_constant__ CUtensorMap map_in, const __grid_constant__ CUtensorMap map_out,
-                      StridedLinesArgs a, Twiddles tw) {
+                      StridedLinesArgs a, Twiddles tw, unsigned first_wait_limit) {
   using L = LinesLaunch<S, WANT>;
   constexpr int G = L::G;
   constexpr int T = S::T, M = S::M, GS = L::GS;
   constexpr int BN = M < 256 ? M : 256;  // elements per box (box: G x BN)
-  constexpr unsigned kLimit = 1u << 22;
+  constexpr unsigned kLimit = 1u << 22;  // try_wait polls before a block gives up
   extern __shared__ __align__(128) float2 smem[];
   float2* stage = smem;  // [M][G] while loading and storing
   uint64_t* bar = reinterpret_cast<uint64_t*>(smem + G * GS);
@@ -180,13 +179,16 @@ __global__ void __launch_bounds__(LinesLaunch<S, WANT>::BLOCK)
           "l"(reinterpret_cast<uint64_t>(&map_in)), "r"(r0), "r"(n0), "r"(mat), "r"(bar_a)
           : "memory");
   }
-  const bool ok = __syncthreads_and(mbar_wait_parity(bar_a, 0, kLimit));
+  const bool ok = __syncthreads_and(mbar_wait_parity(bar_a, 0, first_wait_limit));
   if (!ok) {
-    // give up: record it, wait (bounded) for the copies still in flight
+    // give up: count it for the host (which fails the call), then wait
+    // (bounded, 16x longer) for the copies still in flight before the block
+    // releases its shared memory; its lines are left unwritten
     if (threadIdx.x == 0) {
-      atomicAdd(&g_strided_tma_timeouts, 1u);
-      (void)mbar_wait_parity(bar_a, 0, kLimit);
+      atomicAdd(a.timeouts, 1u);
+      (void)mbar_wait_parity(bar_a, 0, 16u * kLimit);
     }
+    __syncthreads();
     return;
   }
   float2 v[S::R];
@@ -257,6 +259,18 @@ static bool make_lines_map(CUtensorMap* m, const void* base, long long rows, lon
              CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
 }
 
+// Polls of the first input wait before a block gives up.  The full limit
+// unless FFTFREE_TEST_TMA_WAIT_LIMIT is set: a test-only override (0 makes
+// every block give up at once) that exercises the reporting of a wait that
+// ran out; the drain wait keeps its full limit.
+static unsigned first_wait_limit() {
+  static const unsigned lim = [] {
+    const char* e = std::getenv("FFTFREE_TEST_TMA_WAIT_LIMIT");
+    return e ? (unsigned)std::strtoul(e, nullptr, 10) : (1u << 22);
+  }();
+  return lim;
+}
+
 static bool tma_wanted() {
   static const bool on = [] {
     const char* e = std::getenv("FFTFREE_2D_TMA");
@@ -277,7 +291,7 @@ static cudaError_t run_strided_tma(const StridedLinesArgs& a, cudaStream_t st, u
     using L = LinesLaunch<S, WANT>;
     constexpr int G = L::G;
     constexpr int BN = S::M < 256 ? S::M : 256;
-    if (!tma_wanted() || G < 2 || a.rows % G != 0 || (reinterpret_cast<uintptr_t>(a.c.in) & 15) ||
+    if (!tma_wanted() || !a.timeouts || G < 2 || a.rows % G != 0 || (reinterpret_cast<uintptr_t>(a.c.in) & 15) ||
         (reinterpret_cast<uintptr_t>(a.c.out) & 15) || a.rows > 0x7fffffffLL)
       return cudaErrorNotSupported;
     const long long batch = a.c.batch / a.rows;
@@ -295,7 +309,7 @@ static cudaError_t run_strided_tma(const StridedLinesArgs& a, cudaStream_t st, u
     const long long grid = a.c.batch / G;
     if (grid > 0x7fffffffLL) return cudaErrorNotSupported;
     Twiddles tw{twiddle_pyramid(0, st), twiddle_pass_tables(st)};
-    k_fft_strided_tma<S, WANT><<<(unsigned)grid, L::BLOCK, smem, st>>>(mi, mo, a, tw);
+    k_fft_strided_tma<S, WANT><<<(unsigned)grid, L::BLOCK, smem, st>>>(mi, mo, a, tw, first_wait_limit());
     if (launches) ++*launches;
     return cudaGetLastError();
   }

@@ -123,6 +123,10 @@ cudaError_t launch_c2c(const C2cArgs& a, int logr, cudaStream_t s, uint64_t* lau
 struct StridedLinesArgs {
   C2cArgs c;
   long long rows;
+  // TMA route: blocks whose bounded wait for their input boxes gave up add 1
+  // here (the caller zeroes it before the launch and fails the call when it
+  // is non-zero); NULL routes every line through the LSU kernel.
+  unsigned* timeouts = nullptr;
 };
 int max_strided_log();
 cudaError_t launch_c2c_strided(const StridedLinesArgs& a, int logr, cudaStream_t s, uint64_t* launches);

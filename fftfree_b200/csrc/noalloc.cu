@@ -98,8 +98,12 @@ extern "C" FFT_CFFI_API size_t fftfree_execute_complex_batched_noalloc(void* han
                            "memory (host buffers would need staging allocations)\n");
       break;
     }
-    if (ilog2i(N) > max_single_pass_log()) {
-      std::fprintf(stderr, "[fftfree_b200] fftfree_execute_complex_batched_noalloc: N=%d not supported\n", N);
+    // one-pass sizes only (the multi-pass kernels need a scratch chunk): the
+    // half-spectrum C2R path runs an N/2-point transform, the others N points
+    const bool c2r_half_path = c->half_spectrum && c->eff_transform() == 2 && N >= 4;
+    if (ilog2i(N) - (c2r_half_path ? 1 : 0) > max_single_pass_log()) {
+      std::fprintf(stderr, "[fftfree_b200] fftfree_execute_complex_batched_noalloc: N=%d not supported "
+                           "(one-pass sizes only)\n", N);
       break;
     }
     float* frames_buf = out_pcm;

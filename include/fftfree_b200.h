@@ -31,7 +31,12 @@ FFT_CFFI_API int fftfree_execute_c2c(void* handle, const float* in, float* out, 
  * hooks).  `in` / `out` hold batch * rows * cols interleaved complex floats,
  * matrix after matrix; they may alias (the reference works in place).
  * Returns 0 when a context's N does not match its axis (the reference throws
- * std::invalid_argument there), 1 on success.  Runs on ctx_axis0's stream. */
+ * std::invalid_argument there), 1 on success.  Runs on ctx_axis0's stream.
+ * The row pass moves its lines with TMA where the layout allows; its waits for
+ * the copies are bounded, and a block whose wait gives up leaves its lines
+ * unwritten and is counted: a synchronous call then returns 0, an
+ * asynchronous one (fftfree_set_async on device buffers) makes the next
+ * fftfree_execute_2d call on ctx_axis0 return 0. */
 FFT_CFFI_API int fftfree_execute_2d(void* ctx_axis0, void* ctx_axis1, const float* in, float* out, size_t rows,
                                     size_t cols, size_t batch);
 
@@ -92,12 +97,18 @@ FFT_CFFI_API int fftfree_device_available(void);
  * allocates nothing: all three buffers must be device memory (host buffers
  * are rejected, they would need staging), and the per-frame samples that the
  * overlap-add sums are kept in a fixed 16 MiB array compiled into the
- * library, which every GPU that loads the library holds until exit.  Limit:
- * frames * N <= 4,194,304 when the context applies overlap-add; larger calls
- * are rejected with a message on stderr and return 0.  The first call on a
- * device looks up that array's device address (cudaGetSymbolAddress) and
- * should come before any stream capture.  All calls share the array: calls
- * that overlap on the GPU (other streams, other contexts) race on it.
+ * library, which every GPU that loads the library holds until exit.  Limits:
+ * frames * N <= 4,194,304 when the context applies overlap-add, and N up to
+ * 8192 points (16384 for a half-spectrum C2R context), the sizes one pass
+ * covers; other calls are rejected with a message on stderr and return 0.
+ * The first call on a device looks up that array's device address
+ * (cudaGetSymbolAddress) and should come before any stream capture.  With
+ * CUDA's lazy module loading (the default), the first launch of each kernel
+ * loads its code, which may itself take device memory: make one call with
+ * each context (this entry point or fft_execute_complex_batched) before the
+ * time-critical path.  All calls share the array and it keeps the last
+ * call's contents (every sample is rewritten before it is read): calls that
+ * overlap on the GPU (other streams, other contexts) race on it.
  * Returns the frames produced, 0 on failure. */
 FFT_CFFI_API size_t fftfree_execute_complex_batched_noalloc(void* handle, const float* in_real,
                                                            const float* in_imag, size_t frames,

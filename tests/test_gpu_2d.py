@@ -103,3 +103,39 @@ def test_2d_argument_checks():
     assert api.execute_2d(c0, c1, X.view(np.float32), out.view(np.float32), 16, 32, 0) == 0
     assert L.fftfree_execute_2d(None, c1.handle, api._fp(X.view(np.float32)), api._fp(out.view(np.float32)), 16,
                                 32, 1) == 0
+
+
+def test_2d_row_pass_wait_that_gives_up_is_reported():
+    """The TMA row pass bounds its wait for the input boxes; a block whose wait
+    runs out leaves its lines unwritten and the call reports failure.  A
+    test-only limit of 0 polls (FFTFREE_TEST_TMA_WAIT_LIMIT, read once per
+    process, so this runs in a fresh interpreter) makes every block give up
+    at once; the copies still land (the drain wait keeps its full limit).  A
+    synchronous call returns 0; an asynchronous one makes the next call
+    return 0; with the limit unset the same calls succeed."""
+    import os
+    import subprocess
+    import sys
+    repo = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    code = (
+        "import sys, torch; sys.path.insert(0, %r)\n"
+        "import fftfree_b200 as ff\n"
+        "rows, cols, B = 256, 512, 2\n"
+        "c0 = ff.FftContext.full_v2(rows); c1 = ff.FftContext.full_v2(cols)\n"
+        "x = torch.randn(B * rows * cols * 2, device='cuda'); y = torch.empty_like(x)\n"
+        "r_sync = ff.execute_2d(c0, c1, x, y, rows, cols, B)\n"
+        "c0.set_async(True)\n"
+        "r_a1 = ff.execute_2d(c0, c1, x, y, rows, cols, B); torch.cuda.synchronize()\n"
+        "r_a2 = ff.execute_2d(c0, c1, x, y, rows, cols, B); torch.cuda.synchronize()\n"
+        "print('RESULTS', r_sync, r_a1, r_a2)\n" % repo)
+    outs = {}
+    for limit in ("0", None):
+        env = dict(os.environ)
+        env.pop("FFTFREE_TEST_TMA_WAIT_LIMIT", None)
+        if limit is not None:
+            env["FFTFREE_TEST_TMA_WAIT_LIMIT"] = limit
+        r = subprocess.run([sys.executable, "-c", code], capture_output=True, text=True, env=env, timeout=300)
+        assert r.returncode == 0, r.stderr
+        outs[limit] = r.stdout.split("RESULTS", 1)[1].split()
+    assert outs["0"] == ["0", "1", "0"]
+    assert outs[None] == ["1", "1", "1"]
