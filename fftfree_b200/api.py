@@ -97,6 +97,8 @@ _SIGS = [
     ("fftfree_ctx_launch_count", ctypes.c_ulonglong, [ctypes.c_void_p]),
     ("fftfree_ctx_schedule", ctypes.c_int, [ctypes.c_void_p, c_int_p, ctypes.c_int]),
     ("fftfree_ctx_kernel", ctypes.c_int, [ctypes.c_void_p]),
+    ("fftfree_frame_count", ctypes.c_size_t, [ctypes.c_void_p, ctypes.c_size_t, ctypes.c_int, ctypes.c_size_t]),
+    ("fftfree_ctx_frame_shape", ctypes.c_int, [ctypes.c_void_p, c_int_p, c_int_p]),
     ("fftfree_device_available", ctypes.c_int, []),
     ("fftfree_execute_complex_batched_noalloc", ctypes.c_size_t, [ctypes.c_void_p, c_float_p, c_float_p,
                                                                    ctypes.c_size_t, c_float_p, ctypes.c_size_t]),
@@ -147,6 +149,15 @@ def lib() -> ctypes.CDLL:
             fn.argtypes = args
         _lib = L
     return _lib
+
+
+def address(a) -> int:
+    """The address of a numpy array, a torch tensor (host or CUDA) or an int."""
+    if isinstance(a, int):
+        return a
+    if hasattr(a, "data_ptr"):
+        return int(a.data_ptr())
+    return int(a.ctypes.data)
 
 
 def _fp(a) -> ctypes.POINTER(ctypes.c_float):
@@ -228,6 +239,19 @@ class FftContext:
         buf = (ctypes.c_int * 32)()
         n = lib().fftfree_ctx_schedule(self.handle, buf, 32)
         return list(buf[:n])
+
+    def frame_count(self, pcm_len: int, pad_mode: int = 1, max_frames: int = 0) -> int:
+        return int(lib().fftfree_frame_count(self.handle, pcm_len, pad_mode, max_frames))
+
+    def window_length(self) -> int:
+        w, h = ctypes.c_int(0), ctypes.c_int(0)
+        lib().fftfree_ctx_frame_shape(self.handle, ctypes.byref(w), ctypes.byref(h))
+        return int(w.value)
+
+    def hop_length(self) -> int:
+        w, h = ctypes.c_int(0), ctypes.c_int(0)
+        lib().fftfree_ctx_frame_shape(self.handle, ctypes.byref(w), ctypes.byref(h))
+        return int(h.value)
 
     def kernel(self) -> int:
         """Executor code after the FFTFREE_DEFAULT_KERNEL override."""
@@ -322,6 +346,19 @@ class RaggedPlan:
 
     def execute(self, pcm, out_real, out_imag, out_mag) -> int:
         return int(lib().fftfree_ragged_execute(self.handle, _fp(pcm), _fp(out_real), _fp(out_imag), _fp(out_mag)))
+
+    def frame_count(self, pcm_len: int, pad_mode: int = 1, max_frames: int = 0) -> int:
+        return int(lib().fftfree_frame_count(self.handle, pcm_len, pad_mode, max_frames))
+
+    def window_length(self) -> int:
+        w, h = ctypes.c_int(0), ctypes.c_int(0)
+        lib().fftfree_ctx_frame_shape(self.handle, ctypes.byref(w), ctypes.byref(h))
+        return int(w.value)
+
+    def hop_length(self) -> int:
+        w, h = ctypes.c_int(0), ctypes.c_int(0)
+        lib().fftfree_ctx_frame_shape(self.handle, ctypes.byref(w), ctypes.byref(h))
+        return int(h.value)
 
     def kernel(self) -> int:
         """Executor code after the FFTFREE_DEFAULT_KERNEL override."""

@@ -1355,6 +1355,21 @@ FFT_CFFI_API unsigned long long fftfree_ctx_launch_count(void* handle) {
   return c ? (unsigned long long)c->launches : 0ull;
 }
 
+FFT_CFFI_API size_t fftfree_frame_count(void* handle, size_t pcm_len, int pad_mode, size_t max_frames) {
+  FftContext* c = as_ctx(handle);
+  return c ? frame_count(c, pcm_len, pad_mode, max_frames) : 0;
+}
+
+FFT_CFFI_API int fftfree_ctx_frame_shape(void* handle, int* window, int* hop) {
+  FftContext* c = as_ctx(handle);
+  if (!c) return 0;
+  const int W = c->window ? c->window : c->N;
+  const int H = c->hop ? c->hop : W;
+  if (window) *window = W;
+  if (hop) *hop = H;
+  return 1;
+}
+
 FFT_CFFI_API int fftfree_ctx_kernel(void* handle) {
   FftContext* c = as_ctx(handle);
   return c ? c->kernel : -1;

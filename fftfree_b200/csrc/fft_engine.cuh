@@ -192,7 +192,29 @@ struct UntangleTw {
   __device__ __forceinline__ float2 operator()(int i) const {
     return i == 0 ? wt : cmul_rn(wt, wconst<2 * S::R>(i));
   }
+  // w_N^(t + i T) / 2, the factor of the fused untangles: the halving is
+  // folded into the constant (exact), the product taken as two FMAs with
+  // explicit roundings (the same bits in every kernel that inlines it).
+  __device__ __forceinline__ float2 half(int i) const {
+    if (i == 0) return make_float2(0.5f * wt.x, 0.5f * wt.y);
+    const float2 c = wconst<2 * S::R>(i);
+    const float2 h = make_float2(0.5f * c.x, 0.5f * c.y);
+    return make_float2(__fmaf_rn(wt.x, h.x, -__fmul_rn(wt.y, h.y)), __fmaf_rn(wt.x, h.y, __fmul_rn(wt.y, h.x)));
+  }
 };
+
+// Real-input untangle of one bin: with Z the M-point transform of
+// z[m] = x[2m] + i x[2m+1], zk = Z[k], zm = Z[M-k] and h = w_N^k / 2,
+//   X[k] = (zk + conj zm) / 2 + h (-i) (zk - conj zm)
+// in five FMA-class instructions (explicit roundings, no contraction left
+// to the compiler).
+__device__ __forceinline__ float2 untangle_bin(float2 zk, float2 zm, float2 h) {
+  const float2 A = __ffma2_rn(zm, make_float2(1.f, -1.f), zk);   // zk + conj zm
+  const float2 B = __ffma2_rn(zm, make_float2(-1.f, 1.f), zk);   // zk - conj zm
+  // h * (-i B) = h * (B.y, -B.x)
+  const float2 P = make_float2(__fmaf_rn(h.x, B.y, __fmul_rn(h.y, B.x)), __fmaf_rn(h.y, B.y, -__fmul_rn(h.x, B.x)));
+  return __ffma2_rn(A, make_float2(0.5f, 0.5f), P);
+}
 
 // ---------------------------------------------------------------- small DFTs
 // Forward DFT of R points held in v[0 .. R-1], in place, natural order.

@@ -13,11 +13,12 @@
 namespace ffb {
 // ------------------------------------------------------------------ hooks
 // |z| as sqrt(x^2 + y^2): the squares summed with one rounding (fma), then
-// the correctly rounded square root; magnitudes whose squares could
-// overflow fall back to hypotf.
+// s * rsqrt(s) (the hardware reciprocal square root and one multiply, a few
+// ulp) while s is a normal float away from overflow; zero, tiny and huge
+// magnitudes through hypotf.
 __device__ __forceinline__ float cabs_fast(float x, float y) {
-  const float s = fmaf(x, x, y * y);
-  if (s < 1e36f) return __fsqrt_rn(s);
+  const float s = __fmaf_rn(x, x, __fmul_rn(y, y));
+  if (s > 1e-36f && s < 1e36f) return __fmul_rn(s, rsqrtf(s));
   return hypotf(x, y);
 }
 
@@ -111,9 +112,16 @@ __device__ __forceinline__ float2 post_hook(float2 X, int k, int N, const PostFl
   return X;
 }
 
+// (m, phi) -> m e^{i phi}.  Phases in [-pi, pi] (those atan2 produces) use
+// the hardware sine / cosine (absolute error below 2^-21 there); others go
+// through sincos_fast.
 __device__ __forceinline__ float2 polar_to_complex(float2 u) {
   float s, c;
-  sincos_fast(u.y, &s, &c);
+  if (fabsf(u.y) <= 3.14159274f) {
+    __sincosf(u.y, &s, &c);
+  } else {
+    sincos_fast(u.y, &s, &c);
+  }
   return make_float2(u.x * c, u.x * s);
 }
 
@@ -144,6 +152,20 @@ __device__ __forceinline__ float2 unit_phasor(float2 X, float mag) {
   const float s = fmaf(X.x, X.x, X.y * X.y);
   const float r = (s > 1e-36f && s < 1e36f) ? rsqrtf(s) : 1.0f / mag;
   return make_float2(X.x * r, X.y * r);
+}
+
+// |X| and X / |X| from one reciprocal square root (cabs_fast's magnitude,
+// unit_phasor's phasor, bit for bit).
+__device__ __forceinline__ float2 mag_phasor(float2 X, float* mag) {
+  const float s = __fmaf_rn(X.x, X.x, __fmul_rn(X.y, X.y));
+  if (s > 1e-36f && s < 1e36f) {
+    const float r = rsqrtf(s);
+    *mag = __fmul_rn(s, r);
+    return make_float2(X.x * r, X.y * r);
+  }
+  const float m = hypotf(X.x, X.y);
+  *mag = m;
+  return unit_phasor(X, m);
 }
 
 // Frame f of a (possibly multi-signal) STFT: its first sample and how many
@@ -293,17 +315,17 @@ struct StftIO {
       float* pm = mg + t;
 #pragma unroll
       for (int i = 0; i < R; ++i) {
-        const float2 zk = v[i];
         const float2 zm = sm[pidx((M - t - i * T) & (M - 1))];
-        const float2 E = make_float2(0.5f * (zk.x + zm.x), 0.5f * (zk.y - zm.y));
-        const float2 D = make_float2(zk.x - zm.x, zk.y + zm.y);
-        const float2 O = make_float2(0.5f * D.y, -0.5f * D.x);
-        float2 X = cadd(E, cmul_rn(w(i), O));
+        float2 X = untangle_bin(v[i], zm, w.half(i));
         if (i == 0 && t == 0) X.y = 0.f;  // DC
-        if constexpr (MODE >= 3) {
-          const float m = cabs_fast(X.x, X.y);
+        if constexpr (MODE == 4) {
+          float m;
+          reinterpret_cast<float2*>(re)[t + i * T] = mag_phasor(X, &m);
           pm[i * T] = m;
-          if constexpr (MODE == 4) reinterpret_cast<float2*>(re)[t + i * T] = unit_phasor(X, m);
+          continue;
+        }
+        if constexpr (MODE == 3) {
+          pm[i * T] = cabs_fast(X.x, X.y);
           continue;
         }
         float mag;
@@ -547,13 +569,18 @@ struct C2rHalfIO {
       const int m = t + i * T;
       float2 z = make_float2(0.f, 0.f);
       if (ok) {
+        // conj of E + i O, E = (xk + conj xm) / 2, O = (xk - conj xm) conj(w) / 2:
+        // A = xk + conj xm, B = xk - conj xm, Q = B conj(h), h = w / 2,
+        // conj(A / 2 + i Q) = (A.x / 2 - Q.y, -(A.y / 2 + Q.x))
         const float2 xm = sm[pidx(M - m)];
-        const float2 E = make_float2(0.5f * (xk[i].x + xm.x), 0.5f * (xk[i].y - xm.y));
-        const float2 D = make_float2(0.5f * (xk[i].x - xm.x), 0.5f * (xk[i].y + xm.y));
-        const float2 O = cmul_rn(D, cconj(w(i)));
-        z = make_float2(E.x - O.y, E.y + O.x);  // E + i O
+        const float2 A = __ffma2_rn(xm, make_float2(1.f, -1.f), xk[i]);
+        const float2 B = __ffma2_rn(xm, make_float2(-1.f, 1.f), xk[i]);
+        const float2 h = w.half(i);
+        const float2 Q = make_float2(__fmaf_rn(B.x, h.x, __fmul_rn(B.y, h.y)),
+                                     __fmaf_rn(B.y, h.x, -__fmul_rn(B.x, h.y)));
+        z = __ffma2_rn(A, make_float2(0.5f, -0.5f), make_float2(-Q.y, -Q.x));
       }
-      v[i] = cconj(z);  // IDFT via conj . DFT . conj
+      v[i] = z;  // IDFT via conj . DFT . conj: the input already conjugated
     }
     GroupSync::sync<S>();  // the engine reuses the tile
   }

@@ -135,12 +135,15 @@ __device__ __forceinline__ void grad_inverse(const MagGradArgs& a, const float2 
   // the IDFT taken as conj . DFT . conj.
 #pragma unroll
   for (int i = 0; i < R; ++i) {
+    // conj(E + i O) with A = Y[m] + conj Y[M-m], B = Y[m] - conj Y[M-m],
+    // Q = B conj(h), h = w / 2: (A.x / 2 - Q.y, -(A.y / 2 + Q.x))
     const int m = t + i * T;
     const float2 ym = sm[pidx(M - m)];
-    const float2 E = make_float2(0.5f * (y[i].x + ym.x), 0.5f * (y[i].y - ym.y));
-    const float2 D = make_float2(0.5f * (y[i].x - ym.x), 0.5f * (y[i].y + ym.y));
-    const float2 O = cmul(D, cconj(w(i)));
-    v[i] = make_float2(E.x - O.y, -(E.y + O.x));
+    const float2 A = __ffma2_rn(ym, make_float2(1.f, -1.f), y[i]);
+    const float2 B = __ffma2_rn(ym, make_float2(-1.f, 1.f), y[i]);
+    const float2 h = w.half(i);
+    const float2 Q = make_float2(__fmaf_rn(B.x, h.x, __fmul_rn(B.y, h.y)), __fmaf_rn(B.y, h.x, -__fmul_rn(B.x, h.y)));
+    v[i] = __ffma2_rn(A, make_float2(0.5f, -0.5f), make_float2(-Q.y, -Q.x));
   }
   GroupSync::sync<S>();  // the engine reuses the tile
   fft_engine<S, GroupSync>(v, t, sm, tw);
@@ -187,12 +190,8 @@ __device__ __forceinline__ void frame_grad(const MagGradArgs& a, const float* pc
 #pragma unroll
   for (int i = 0; i < R; ++i) {
     const int k = t + i * T;
-    const float2 zk = v[i];
     const float2 zm = sm[pidx((M - k) & (M - 1))];
-    const float2 E = make_float2(0.5f * (zk.x + zm.x), 0.5f * (zk.y - zm.y));
-    const float2 D = make_float2(zk.x - zm.x, zk.y + zm.y);
-    const float2 O = make_float2(0.5f * D.y, -0.5f * D.x);
-    float2 X = cadd(E, cmul_rn(w(i), O));
+    float2 X = untangle_bin(v[i], zm, w.half(i));
     if (i == 0 && t == 0) {
       X.y = 0.f;  // DC is real
       const float2 V = mag_chain(X, gk[0]);

@@ -86,6 +86,13 @@ FFT_CFFI_API int fftfree_ctx_schedule(void* handle, int* radices, int max_passes
  * (Cooley-Tukey), 1 Cooley-Tukey, 2 Stockham; -1 for a NULL handle. */
 FFT_CFFI_API int fftfree_ctx_kernel(void* handle);
 
+/* Frames fft_execute_batched would produce for pcm_len samples with this
+ * pad_mode and max_frames (the rule of fft_cffi.cpp:710-750), and the
+ * context's effective frame length W and hop H (window / hop, 0 -> N / W):
+ * what a caller needs to split one signal's frames over several GPUs. */
+FFT_CFFI_API size_t fftfree_frame_count(void* handle, size_t pcm_len, int pad_mode, size_t max_frames);
+FFT_CFFI_API int fftfree_ctx_frame_shape(void* handle, int* window, int* hop);
+
 /* 1 when a CUDA device is usable by this library, else 0. */
 FFT_CFFI_API int fftfree_device_available(void);
 

@@ -114,6 +114,7 @@ def test_backup_batched_against_reference(observer, name, setup, frames, N, W, H
     o = oracle_for(kw)
     assert o.frame_count(len(pcm), 1) == frames
     given_up = _given_up(setup, frames)
+    observer.clear()  # the debug plan reported to the same observer
     L = ff.lib()
     _reset(L)
     setup(L)
@@ -148,6 +149,7 @@ def test_backup_complex_batched_against_reference(observer, name, setup, frames)
     ri = rng.standard_normal(frames * bins).astype(np.float32)
     ii = rng.standard_normal(frames * bins).astype(np.float32)
     given_up = _given_up(setup, frames)
+    observer.clear()  # the debug plan reported to the same observer
     L = ff.lib()
     _reset(L)
     setup(L)
