@@ -118,6 +118,10 @@ _SIGS = [
                                                                 ctypes.c_size_t, c_float_p, c_float_p]),
     ("fftfree_ragged_plan", ctypes.c_void_p, [ctypes.POINTER(ctypes.c_size_t), ctypes.c_size_t, ctypes.c_int,
                                               ctypes.c_int]),
+    ("fftfree_ragged_plan_stft", ctypes.c_void_p, [ctypes.POINTER(ctypes.c_size_t), ctypes.POINTER(ctypes.c_size_t),
+                                                   c_int_p, c_int_p, c_int_p, c_float_p, ctypes.c_size_t,
+                                                   ctypes.c_int, ctypes.c_int]),
+    ("fftfree_ragged_frames", ctypes.c_size_t, [ctypes.c_void_p, ctypes.c_size_t]),
     ("fftfree_ragged_samples", ctypes.c_size_t, [ctypes.c_void_p]),
     ("fftfree_ragged_bins", ctypes.c_size_t, [ctypes.c_void_p]),
     ("fftfree_ragged_schedule", ctypes.c_int, [ctypes.c_void_p, ctypes.c_size_t]),
@@ -323,12 +327,32 @@ class RaggedPlan:
     """One persistent launch over real signals of mixed sizes (see
     fftfree_ragged_plan in include/fftfree_b200.h)."""
 
-    def __init__(self, sizes, reduce_magnitude=0, store_polar=0):
+    def __init__(self, sizes, reduce_magnitude=0, store_polar=0, lengths=None, window=None, hop=None,
+                 window_kind=None, window_param=None):
+        """sizes: transform size N of each item.  With only sizes, item i is one
+        frame of N samples; with ``lengths`` (samples per signal) and optional
+        per-item ``window`` / ``hop`` / ``window_kind`` / ``window_param`` the
+        items are framed signals (fftfree_ragged_plan_stft)."""
         self.sizes = [int(n) for n in sizes]
-        arr = (ctypes.c_size_t * len(self.sizes))(*self.sizes)
-        self.handle = lib().fftfree_ragged_plan(arr, len(self.sizes), reduce_magnitude, store_polar)
+        cnt = len(self.sizes)
+        arr = (ctypes.c_size_t * cnt)(*self.sizes)
+        if lengths is None and window is None and hop is None and window_kind is None:
+            self.handle = lib().fftfree_ragged_plan(arr, cnt, reduce_magnitude, store_polar)
+        else:
+            lens = (ctypes.c_size_t * cnt)(*[int(v) for v in (lengths if lengths is not None else self.sizes)])
+
+            def ints(seq):
+                return None if seq is None else ctypes.cast((ctypes.c_int * cnt)(*[int(v) for v in seq]), c_int_p)
+
+            params = None if window_param is None else ctypes.cast(
+                (ctypes.c_float * cnt)(*[float(v) for v in window_param]), c_float_p)
+            self.handle = lib().fftfree_ragged_plan_stft(arr, lens, ints(window), ints(hop), ints(window_kind),
+                                                         params, cnt, reduce_magnitude, store_polar)
         if not self.handle:
             raise RuntimeError("fftfree_ragged_plan failed")
+
+    def frames(self, item: int) -> int:
+        return int(lib().fftfree_ragged_frames(self.handle, item))
 
     @property
     def samples(self) -> int:

@@ -223,6 +223,12 @@ static std::vector<float> build_window(int kind, int W, float p1, float /*p2*/) 
   return w;
 }
 
+std::vector<float> window_taps(int kind, int W, float p1, float p2, int norm_policy) {
+  std::vector<float> w = build_window(kind, W, p1, p2);
+  normalize_window(w, norm_policy);
+  return w;
+}
+
 static void upload_windows(FftContext* c) {
   if (!c->windows_enabled || c->windows_uploaded) return;
   const size_t n = (size_t)c->N;

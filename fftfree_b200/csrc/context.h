@@ -97,4 +97,8 @@ struct FftContext {
 
 FftContext* as_ctx(void* h);
 
+// The W taps of an analysis / synthesis window as the contexts build them
+// (fft_cffi.cpp:163-208: kind, parameter p1, normalisation policy).
+std::vector<float> window_taps(int kind, int W, float p1, float p2, int norm_policy);
+
 }  // namespace ffb

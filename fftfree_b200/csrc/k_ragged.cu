@@ -1,168 +1,176 @@
 // k_ragged.cu -- one persistent launch over a ragged batch of real
-// transforms (R2C, half spectrum) of different sizes.
+// transforms (R2C, half spectrum) of different sizes and framings.
 //
-// Each item i is a signal of N_i = 2^L samples transformed as one full
-// frame (window = hop = N_i), exactly as fft_execute_batched does for a
-// context of that size (fft_cffi.cpp:701-824); outputs are the planar
-// (re, im, mag) rows of N_i/2 + 1 bins, concatenated in item order.
-//
-// The host builds a work list of tiles, largest first (longest processing
-// time first balances the persistent blocks): a tile is either a group of
-// same-size items of up to 2^12 complex points, one per S::T-thread slice
-// of the 256-thread block (the single-pass engine and the STFT load/store
-// policy, so these items match fft_execute_batched bit for bit), or one
-// item of 2^13 .. 2^15 complex points, which the block transforms in three
-// phases through its own global scratch (columns, rows, untangle; one slot
-// of 2^15 points per block, rewritten in place).  Blocks
-// take tiles from an atomic counter until the list is exhausted.
+// Item i is a signal framed as fft_execute_batched frames it (pad_mode 1,
+// fft_cffi.cpp:701-824): frames of W_i samples at hop H_i, zero-padded to
+// N_i, windowed by the item's analysis taps; its frames' planar (re, im,
+// mag) rows of N_i/2 + 1 bins are concatenated in item order.  Every frame
+// is one job; the host groups the jobs of one size into tiles, largest
+// first (longest processing time first balances the persistent blocks), and
+// the blocks (1024 threads, one per SM) take tiles from an atomic counter
+// until the list is exhausted.  A tile is
+//  * a group of same-size frames of up to 2^14 complex points, one per
+//    T-thread slice of the block -- the single-pass engine and the STFT
+//    load / store policy of fft_execute_batched, so a frame matches that
+//    call bit for bit where the radix is the same; 2^14 points take the
+//    whole block (T = 1024, the transform held in registers and 139 KB of
+//    shared memory);
+//  * one frame of 2^15 complex points (N = 65536), which exceeds one SM's
+//    shared memory: a decimation-in-time split into two 2^14-point
+//    transforms of the even and odd points, run one after the other through
+//    the block's engine; the first half's spectrum waits in a 128 KB scratch
+//    slot of the block (148 slots, 19 MB: L2-resident), and the combine step
+//    untangles bins k and k + M/2 together so the outputs stay contiguous.
 #include "fft_launch.cuh"
 
 namespace ffb {
 namespace {
 
-constexpr int kBlock = 256;
-constexpr int kLargeMin = 13, kLargeMax = 15;  // log2 complex points of the three-phase path
-
-template <class S>
-__host__ __device__ constexpr int rtile() {
-  return ((S::SMEM + 15) / 16) * 16 + 1;  // 1 mod 16: lanes on different tiles, different banks
-}
+constexpr int kBlock = 1024;
+constexpr int kSplitLog = 15;  // log2 complex points of the two-half path
+constexpr int kFullLog = 14;   // one-block single pass
 
 // ---------------------------------------------------------------- single-pass tile
 template <class S, int MODE>
 __device__ __forceinline__ void ragged_single(const RaggedArgs& a, int4 tile, float2* smem, const Twiddles& tw) {
   constexpr int T = S::T;
+  static_assert(T <= 32 || kBlock / T <= 15 || T >= 256, "named barrier per group");
   const int g = threadIdx.x / T;
   const int t = threadIdx.x - g * T;
   const bool ok = g < tile.y;
-  const int item = tile.x + (ok ? g : 0);
-  const long long po = __ldg(a.pcm_off + item), oo = __ldg(a.out_off + item);
+  const int2 job = __ldg(a.jobs + tile.x + (ok ? g : 0));
+  const RaggedItem it = a.items[job.x];
   StftArgs sa{};
-  sa.pcm = a.pcm + po;
-  sa.pcm_len = 2LL * S::M;
-  sa.frames = ok ? 1 : 0;
+  sa.pcm = a.pcm + it.pcm_off;
+  sa.pcm_len = it.pcm_len;
+  sa.frames = ok ? (long long)job.y + 1 : 0;  // frame job.y of the item (none when !ok)
   sa.N = 2 * S::M;
-  sa.W = sa.N;
-  sa.H = sa.N;
+  sa.W = it.W;
+  sa.H = it.H;
+  sa.win = it.win_off >= 0 ? a.windows + it.win_off : nullptr;
   sa.pf = a.pf;
   sa.out_bins = S::M + 1;
   sa.out_stride = S::M + 1;
   sa.mag_from_real = 1;
-  sa.out_re = a.out_re + oo;
-  sa.out_im = a.out_im + oo;
-  sa.out_mag = a.out_mag + oo;
+  sa.out_re = a.out_re + it.out_off;
+  sa.out_im = a.out_im + it.out_off;
+  sa.out_mag = a.out_mag + it.out_off;
   const StftIO<MODE> io{sa, S::LOGM + 1};
   float2* sm = smem + g * S::SMEM;
   float2 v[S::R];
-  io.template load<S>(0, t, v, sm, tw);
+  io.template load<S>(job.y, t, v, sm, tw);
   fft_engine<S, GroupSync>(v, t, sm, tw);
-  io.template store<S>(0, t, v, sm, tw);
+  io.template store<S>(job.y, t, v, sm, tw);
 }
 
-// ---------------------------------------------------------------- three-phase tile
-// z[m] = (x[2m], x[2m+1]), M = M1 * M2 points, m = n1 M2 + n2, k = k1 + M1 k2.
-template <int LM1, int LM2, int MODE>
-__device__ __forceinline__ void ragged_large(const RaggedArgs& a, int4 tile, float2* smem, const Twiddles& tw) {
-  constexpr int LM = LM1 + LM2, M = 1 << LM, M1 = 1 << LM1, M2 = 1 << LM2;
-  using SA = Sched<LM1, LM1 - 4>;  // 16 threads per column
-  using SB = Sched<LM2, LM2 - 4>;  // 16 threads per row
-  static_assert(SA::T == 16 && SB::T == 16, "16 threads per sub-transform");
-  const int item = tile.x;
-  const float* x = a.pcm + __ldg(a.pcm_off + item);
-  const long long oo = __ldg(a.out_off + item);
-  // one slot of M points per block: phase A writes the columns' results in
-  // row order, phase B overwrites each group of 16 rows, in place, with their
-  // results in [k2][row] order (contiguous stores), phase C reads Z[k] at
-  // zidx(k).  (A slot per block of M points keeps all blocks' scratch,
-  // 444 x 256 KiB, inside the 126 MB L2.)
-  float2* scr_a = a.scratch + (long long)blockIdx.x * (1LL << kLargeMax);
-  const auto zidx = [](int k) -> long long {
-    const int k1 = k & (M1 - 1), k2 = k >> LM1;
-    return (long long)(k1 >> 4) * 16 * M2 + (long long)k2 * 16 + (k1 & 15);
-  };
-  float2* tiles = smem;
-  float2* stage = smem + 16 * rtile<SA>();
-  // phase A: 16 columns at a time, 16 threads each (lanes walk n2)
-  {
-    const bool x8 = (reinterpret_cast<uintptr_t>(x) & 7) == 0;
-    const int c = threadIdx.x & 15, t = threadIdx.x >> 4;
+// ---------------------------------------------------------------- two-half tile
+// Samples j, j + 1 of the windowed, zero-padded frame.
+__device__ __forceinline__ float2 frame_pair(const float* src, const float* win, long long cnt, long long j,
+                                             bool fast) {
+  if (fast) {
+    float2 z = __ldg(reinterpret_cast<const float2*>(src + j));
+    if (win) z = __fmul2_rn(z, __ldg(reinterpret_cast<const float2*>(win + j)));
+    return z;
+  }
+  float x0 = 0.f, x1 = 0.f;
+  if (j < cnt) x0 = win ? __ldg(src + j) * __ldg(win + j) : __ldg(src + j);
+  if (j + 1 < cnt) x1 = win ? __ldg(src + j + 1) * __ldg(win + j + 1) : __ldg(src + j + 1);
+  return make_float2(x0, x1);
+}
+
+// M = 2^15 complex points z[m] = (s[2m], s[2m+1]) of an N = 2^16 frame:
+// E = DFT_{M/2}(z[2n]), O = DFT_{M/2}(z[2n+1]),
+// Z[k] = E[k] + w_M^k O[k], Z[k + M/2] = E[k] - w_M^k O[k]; then
+// X[k] = untangle(Z[k], Z[M - k]) and X[k + M/2] = untangle(Z[k + M/2], Z[M/2 - k]).
+// The points z[2n + odd] of the tile's frame into v (n = t + i T).  The
+// frame's bookkeeping is re-read for each half, so that nothing but the tile
+// stays live across the engine (a 2^14-point engine at 1024 threads uses the
+// whole register budget).
+template <class S>
+__device__ __forceinline__ void split_load(const RaggedArgs& a, int4 tile, int odd, int t, float2 (&v)[S::R]) {
+  constexpr int T = S::T, R = S::R, N = 4 * S::M;
+  const int2 job = __ldg(a.jobs + tile.x);
+  const RaggedItem it = a.items[job.x];
+  long long cnt;
+  const float* src = stft_frame(a.pcm + it.pcm_off, it.pcm_len, 0, 0, it.W, it.H, job.y, &cnt);
+  const float* win = it.win_off >= 0 ? a.windows + it.win_off : nullptr;
+  const bool fast = cnt == (long long)N && aligned8(src) && (!win || aligned8(win));
+#pragma unroll
+  for (int i = 0; i < R; ++i) v[i] = frame_pair(src, win, cnt, 4LL * (t + i * T) + 2 * odd, fast);
+}
+
+template <int MODE>
+__device__ __forceinline__ void ragged_split(const RaggedArgs& a, int4 tile, float2* smem, const Twiddles& tw) {
+  using S = Sched<kSplitLog - 1, 4>;
+  constexpr int T = S::T, R = S::R, MH = S::M, M = 2 * MH, LM = kSplitLog;
+  static_assert(T == kBlock, "the whole block per half");
+  const int t = threadIdx.x;
+
+  // even points: E, into the block's scratch slot; then the odd points: O,
+  // into the tile (the engine's barriers also order the scratch writes
+  // before the combine's reads).  One engine body for both halves.
 #pragma unroll 1
-    for (int c0 = 0; c0 < M2; c0 += 16) {
-      const int n2 = c0 + c;
-      float2 v[SA::R];
-      if (x8) {  // z[m] = (x[2m], x[2m+1]) as one 8-byte load
-        const float2* x2 = reinterpret_cast<const float2*>(x);
+  for (int odd = 0; odd < 2; ++odd) {
+    float2 v[R];
+    split_load<S>(a, tile, odd, t, v);
+    fft_engine<S, GroupSync>(v, t, smem, tw);
+    if (odd) {
+      tile_write_natural<S>(v, t, smem);
+    } else {
+      float2* scr = a.scratch + (long long)blockIdx.x * MH;
 #pragma unroll
-        for (int i = 0; i < SA::R; ++i) v[i] = __ldg(x2 + (long long)(t + 16 * i) * M2 + n2);
-      } else {
-#pragma unroll
-        for (int i = 0; i < SA::R; ++i) {
-          const long long m = (long long)(t + 16 * i) * M2 + n2;
-          v[i] = make_float2(__ldg(x + 2 * m), __ldg(x + 2 * m + 1));
-        }
-      }
-      fft_engine<SA, BlockSync>(v, t, tiles + c * rtile<SA>(), tw);
-#pragma unroll
-      for (int i = 0; i < SA::R; ++i) {
-        const int k1 = t + 16 * i;
-        scr_a[(long long)k1 * M2 + n2] = cmul(v[i], tw_split(tw, LM, (unsigned)(n2 * k1)));
-      }
+      for (int i = 0; i < R; ++i) scr[t + i * T] = v[i];
     }
   }
   __syncthreads();
-  // phase B: 16 rows at a time, 16 consecutive lanes per row (lanes walk n2);
-  // results staged so that the writes of Z[k1 + M1 k2] walk k1
-  {
-    const int j = threadIdx.x >> 4, t = threadIdx.x & 15;
-#pragma unroll 1
-    for (int r0 = 0; r0 < M1; r0 += 16) {
-      const int k1 = r0 + j;
-      float2 v[SB::R];
-#pragma unroll
-      for (int i = 0; i < SB::R; ++i) v[i] = scr_a[(long long)k1 * M2 + t + 16 * i];
-      fft_engine<SB, BlockSync>(v, t, tiles + j * rtile<SB>(), tw);
-#pragma unroll
-      for (int i = 0; i < SB::R; ++i) stage[(t + 16 * i) * 17 + j] = v[i];
-      __syncthreads();
-      // rows r0 .. r0+15 are in registers: their region takes the results
-      for (int flat = threadIdx.x; flat < 16 * M2; flat += kBlock) {
-        const int k2 = flat >> 4, jj = flat & 15;
-        scr_a[(long long)r0 * M2 + flat] = stage[k2 * 17 + jj];
-      }
-      __syncthreads();
-    }
-  }
-  // phase C: untangle X[k] = E + w_N^k O from Z[k], Z[M - k]; post hook and
-  // planar stores as fft_execute_batched's epilogue (fft_cffi.cpp:813-824)
+
+  const int2 job = __ldg(a.jobs + tile.x);
+  const RaggedItem it = a.items[job.x];
+  const float2* scr = a.scratch + (long long)blockIdx.x * MH;
+
   StftArgs sa{};
   sa.N = 2 * M;
   sa.pf = a.pf;
   sa.mag_from_real = 1;
   const StftIO<MODE> io{sa, LM + 1};
   const bool mag_is_re = (MODE == 1) || (MODE == 2);
-  float* re = a.out_re + oo;
-  float* im = a.out_im + oo;
-  float* mg = a.out_mag + oo;
-  const float2* w = tw.pyr + ((2u << LM) - 1u);  // level log2 N
-  for (int k = threadIdx.x; k <= M; k += kBlock) {
-    if (k == M) {
-      const float2 z0 = scr_a[zidx(0)];
-      io.emit(re, im, mg, M, make_float2(z0.x - z0.y, 0.f), true, 1.0f, mag_is_re);
-      continue;
+  float* re = a.out_re + it.out_off + (long long)job.y * (M + 1);
+  float* im = a.out_im + it.out_off + (long long)job.y * (M + 1);
+  float* mg = a.out_mag + it.out_off + (long long)job.y * (M + 1);
+#pragma unroll 2
+  for (int i = 0; i < R; ++i) {
+    const int k = t + i * T;
+    const float2 wk = tw_get(tw, LM, (unsigned)k);      // w_M^k
+    const float2 e = scr[k];
+    const float2 o = cmul(smem[pidx(k)], wk);  // O[k] (from the tile: the registers go to the combine)
+    const float2 zk = cadd(e, o);                       // Z[k]
+    const float2 zk2 = csub(e, o);                      // Z[k + M/2]
+    float2 zmk, zmk2;                                   // Z[M - k], Z[M/2 - k]
+    if (k == 0) {
+      zmk = zk;
+      zmk2 = zk2;
+    } else {
+      const float2 wm = make_float2(-wk.x, wk.y);       // w_M^(M/2 - k) = -conj(w_M^k)
+      const float2 om = cmul(smem[pidx(MH - k)], wm);
+      const float2 em = scr[MH - k];
+      zmk2 = cadd(em, om);
+      zmk = csub(em, om);
     }
-    const float2 zk = scr_a[zidx(k)];
-    const float2 zm = scr_a[zidx((M - k) & (M - 1))];
-    const float2 E = make_float2(0.5f * (zk.x + zm.x), 0.5f * (zk.y - zm.y));
-    const float2 D = make_float2(zk.x - zm.x, zk.y + zm.y);
-    const float2 O = make_float2(0.5f * D.y, -0.5f * D.x);
-    const float2 X = cadd(E, cmul(__ldg(w + k), O));
+    const float2 wn = tw_get(tw, LM + 1, (unsigned)k);  // w_N^k
+    const float2 h = make_float2(0.5f * wn.x, 0.5f * wn.y);
+    const float2 h2 = make_float2(0.5f * wn.y, -0.5f * wn.x);  // w_N^(k + M/2) / 2 = -i w_N^k / 2
+    float2 X = untangle_bin(zk, zmk, h);
+    if (k == 0) X.y = 0.f;  // DC
     io.emit(re, im, mg, k, X, k == 0, 1.0f, mag_is_re);
+    io.emit(re, im, mg, k + MH, untangle_bin(zk2, zmk2, h2), false, 1.0f, mag_is_re);
+    if (k == 0) io.emit(re, im, mg, M, make_float2(zk.x - zk.y, 0.f), true, 1.0f, mag_is_re);  // Nyquist
   }
-  __syncthreads();  // scratch and tiles are reused by the block's next tile
+  __syncthreads();  // shared memory and scratch are reused by the block's next tile
 }
 
 // ---------------------------------------------------------------- dispatch
-// tile.z = log2 complex points, tile.w = pass radix (log2) of a single-pass tile.
+// tile.z = log2 complex points, tile.w = pass radix (log2); the pass radices
+// keep T = M / R out of (32, 128) (named barriers per group: 15 at most).
 template <int MODE>
 __device__ __forceinline__ void ragged_tile(const RaggedArgs& a, int4 tile, float2* smem, const Twiddles& tw) {
 #define FFB_RS(L, R)                                              \
@@ -172,18 +180,16 @@ __device__ __forceinline__ void ragged_tile(const RaggedArgs& a, int4 tile, floa
   switch (tile.z * 8 + tile.w) {
     FFB_RS(1, 2) FFB_RS(2, 2) FFB_RS(3, 2) FFB_RS(4, 2)
     FFB_RS(5, 2) FFB_RS(5, 3) FFB_RS(6, 3) FFB_RS(6, 4) FFB_RS(7, 3) FFB_RS(7, 4)
-    FFB_RS(8, 3) FFB_RS(8, 4) FFB_RS(9, 3) FFB_RS(9, 4) FFB_RS(10, 3) FFB_RS(10, 4)
-    FFB_RS(11, 3) FFB_RS(11, 4) FFB_RS(12, 4)
-    case 13 * 8: ragged_large<7, 6, MODE>(a, tile, smem, tw); return;
-    case 14 * 8: ragged_large<7, 7, MODE>(a, tile, smem, tw); return;
-    case 15 * 8: ragged_large<8, 7, MODE>(a, tile, smem, tw); return;
+    FFB_RS(8, 3) FFB_RS(8, 4) FFB_RS(9, 4) FFB_RS(10, 3)
+    FFB_RS(11, 3) FFB_RS(11, 4) FFB_RS(12, 4) FFB_RS(13, 4) FFB_RS(14, 4)
+    case kSplitLog * 8: ragged_split<MODE>(a, tile, smem, tw); return;
     default: return;
   }
 #undef FFB_RS
 }
 
 template <int MODE>
-__global__ void __launch_bounds__(kBlock, 3) k_ragged(RaggedArgs a, Twiddles tw) {
+__global__ void __launch_bounds__(kBlock, 1) k_ragged(RaggedArgs a, Twiddles tw) {
   extern __shared__ float2 smem[];
   __shared__ int next;
   for (;;) {
@@ -196,20 +202,31 @@ __global__ void __launch_bounds__(kBlock, 3) k_ragged(RaggedArgs a, Twiddles tw)
   }
 }
 
-constexpr size_t ragged_smem_bytes() {
-  // single-pass: one 256-thread tile of at most 2^12 points; three-phase:
-  // 16 column / row tiles of up to 256 points plus the 128 x 17 staging
-  constexpr size_t single = (size_t)4608 * sizeof(float2);  // max over sizes of (256 / T) * S::SMEM
-  constexpr size_t large = (size_t)(16 * rtile<Sched<8, 4>>() + 128 * 17) * sizeof(float2);
-  return single > large ? single : large;
+// Shared memory of a tile of (L, R): one padded tile per T-thread group.
+template <int L, int R>
+constexpr size_t tile_smem() {
+  using S = Sched<L, R>;
+  return (size_t)(kBlock / S::T) * S::SMEM * sizeof(float2);
 }
+constexpr size_t cmax(size_t a, size_t b) { return a > b ? a : b; }
+
+constexpr size_t ragged_smem_bytes() {
+  // the largest over the tiles of ragged_tile (small transforms carry more
+  // padding per point: 256 groups of 64 points take the most)
+  return cmax(cmax(cmax(cmax(tile_smem<1, 2>(), tile_smem<2, 2>()), cmax(tile_smem<3, 2>(), tile_smem<4, 2>())),
+                   cmax(cmax(tile_smem<5, 2>(), tile_smem<5, 3>()), cmax(tile_smem<6, 3>(), tile_smem<6, 4>()))),
+              cmax(cmax(cmax(tile_smem<7, 3>(), tile_smem<7, 4>()), cmax(tile_smem<8, 3>(), tile_smem<8, 4>())),
+                   cmax(cmax(cmax(tile_smem<9, 4>(), tile_smem<10, 3>()), cmax(tile_smem<11, 3>(), tile_smem<11, 4>())),
+                        cmax(cmax(tile_smem<12, 4>(), tile_smem<13, 4>()), tile_smem<14, 4>()))));
+}
+static_assert(ragged_smem_bytes() <= 227 * 1024, "one block per SM");
 
 template <int MODE>
 cudaError_t launch_mode(const RaggedArgs& a, int grid, cudaStream_t st, uint64_t* launches) {
   const size_t smem = ragged_smem_bytes();
   cudaError_t e = cudaFuncSetAttribute(k_ragged<MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
-  Twiddles tw{twiddle_pyramid(kLargeMax + 1, st), twiddle_pass_tables(st)};
+  Twiddles tw{twiddle_pyramid(kSplitLog + 1, st), twiddle_pass_tables(st)};
   k_ragged<MODE><<<grid, kBlock, smem, st>>>(a, tw);
   if (launches) ++*launches;
   return cudaGetLastError();
@@ -217,15 +234,18 @@ cudaError_t launch_mode(const RaggedArgs& a, int grid, cudaStream_t st, uint64_t
 
 }  // namespace
 
-int ragged_max_log() { return kLargeMax + 1; }  // log2 N of the largest item
-bool ragged_large_log(int logm) { return logm >= kLargeMin && logm <= kLargeMax; }
-size_t ragged_scratch_per_block() { return (1ull << kLargeMax) * sizeof(float2); }
+int ragged_max_log() { return kSplitLog + 1; }  // log2 N of the largest item
+int ragged_block_log(int logm) { return logm >= kFullLog ? 1 : 0; }
+size_t ragged_scratch_per_block() { return (size_t)(1u << (kSplitLog - 1)) * sizeof(float2); }
+int ragged_block_threads() { return kBlock; }
 
 int ragged_candidates(int logm, int* lrs) {
-  if (logm >= kLargeMin) return 0;
+  if (logm >= kSplitLog) return 0;
   if (logm <= 4) { lrs[0] = 2; return 1; }
   if (logm == 5) { lrs[0] = 2; lrs[1] = 3; return 2; }
-  if (logm == 12) { lrs[0] = 4; return 1; }
+  if (logm == 9) { lrs[0] = 4; return 1; }   // T = 32 (radix 8 would give T = 64)
+  if (logm == 10) { lrs[0] = 3; return 1; }  // T = 128 (radix 16 would give T = 64)
+  if (logm >= 12) { lrs[0] = 4; return 1; }
   lrs[0] = 3;
   lrs[1] = 4;
   return 2;

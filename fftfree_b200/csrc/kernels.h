@@ -177,24 +177,38 @@ cudaError_t launch_stft_mag_grad(const MagGradArgs& a, int logr, cudaStream_t s,
 // half spectrum, one full frame per item).  tiles[i] = {first item, items,
 // log2 complex points, pass radix (log2; 0 for the three-phase sizes)};
 // items are listed in tile order, with their signal and output offsets.
+// One item of a ragged batch: a real signal of pcm_len samples framed as
+// fft_execute_batched frames it with pad_mode 1 (fft_cffi.cpp:710-791:
+// frame f covers f*H .. f*H + W, zero-padded to N), its frames' half
+// spectra (N/2 + 1 bins each, frame-major) from out_off on.
+struct RaggedItem {
+  long long pcm_off;  // first sample of the signal in RaggedArgs::pcm
+  long long pcm_len;  // samples of the signal
+  long long out_off;  // first bin of its first frame in the outputs
+  int W, H;           // frame length (<= N) and hop
+  int win_off;        // analysis window taps at windows + win_off, -1 for none
+  int pad_;
+};
 struct RaggedArgs {
   const float* pcm;
   float* out_re;
   float* out_im;
   float* out_mag;
-  const long long* pcm_off;
-  const long long* out_off;
-  const int4* tiles;
+  const RaggedItem* items;
+  const int2* jobs;     // (item, frame) per frame, tiles' jobs contiguous
+  const int4* tiles;    // x first job, y jobs, z log2 of N/2, w pass radix (log2) or 0 (one-block paths)
   int ntiles;
-  int* counter;     // tiles handed out; zero before each launch
-  float2* scratch;  // ragged_scratch_per_block() bytes per block
+  int* counter;         // tiles handed out; zero before each launch
+  float2* scratch;      // ragged_scratch_per_block() bytes per block
+  const float* windows; // analysis window taps of every item, concatenated
   PostFlags pf;
 };
 int ragged_max_log();                 // largest log2 N
-bool ragged_large_log(int logm);      // sizes that take the three-phase path
+int ragged_block_log(int logm);       // sizes one block takes alone: 1, else 0
 size_t ragged_scratch_per_block();
-int ragged_candidates(int logm, int* lrs);  // pass radices (log2) a size may use; 0 for three-phase
+int ragged_candidates(int logm, int* lrs);  // pass radices (log2) a size may use
 int ragged_grid();                    // persistent blocks for the current device
+int ragged_block_threads();           // threads per block of the persistent kernel
 cudaError_t launch_ragged(const RaggedArgs& a, int grid, cudaStream_t s, uint64_t* launches);
 
 // Multi-pass (four-step) transforms for 2^14 <= N <= 2^20.  `scratch` holds

@@ -1,14 +1,14 @@
-// ragged.cpp -- ragged batches of real transforms of mixed sizes in one
-// persistent launch: the work list, the per-size schedule autotuner and its
-// on-disk cache, the CUDA graph of the launch, and the C ABI
-// (fftfree_ragged_*).
+// ragged.cpp -- ragged batches of real transforms of mixed sizes and
+// framings in one persistent launch: the work list, the per-size schedule
+// autotuner and its on-disk cache, the CUDA graph of the launch, and the C
+// ABI (fftfree_ragged_*).
 //
 // The reference has no ragged entry point: its callers create one context
-// per transform size and loop over the transforms (fft_init_full +
+// per transform size and framing and loop over the signals (fft_init_full +
 // fft_execute_batched per size).  An item here gives the same outputs as
-// fft_execute_batched on a context (n_i, window = hop = n_i, transform = R2C,
-// half_spectrum = 1, reduce_magnitude / store_polar as the plan's flags)
-// for one frame of n_i samples.
+// fft_execute_batched with pad_mode 1 on a context (n_i, window W_i, hop H_i,
+// transform = R2C, half_spectrum = 1, the item's analysis window,
+// reduce_magnitude / store_polar as the plan's flags) for its signal.
 #include <cuda_runtime.h>
 #include <sys/stat.h>
 
@@ -23,6 +23,7 @@
 #include <tuple>
 #include <vector>
 
+#include "../../include/fft_cffi.h"
 #include "../../include/fftfree_b200.h"
 #include "context.h"
 #include "kernels.h"
@@ -38,12 +39,14 @@ struct RaggedPlan {
   cudaStream_t own_stream = nullptr;
   cudaStream_t stream = nullptr;
   std::vector<int> logm;               // per item (caller order): log2 of N/2
-  std::vector<long long> in_off, out_off;  // per item (caller order)
+  std::vector<RaggedItem> items;       // per item (caller order)
+  std::vector<long long> frames;       // per item
+  std::vector<float> windows;          // analysis taps, items' win_off into it
   size_t samples = 0, bins = 0;
   PostFlags pf{};
   int lr[16] = {};                     // pass radix (log2) per log2 N/2 of the single-pass sizes
   int grid = 0, ntiles = 0;
-  DevBuf d_pcm_off, d_out_off, d_tiles, d_counter, d_scratch, d_in, d_re, d_im, d_mag;
+  DevBuf d_items, d_jobs, d_tiles, d_counter, d_scratch, d_windows, d_in, d_re, d_im, d_mag;
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t exec = nullptr;
   const void* graph_ptrs[4] = {};
@@ -83,40 +86,37 @@ bool is_device(const void* p) {
 }
 
 // ---------------------------------------------------------------- work list
-// Tiles of same-size items in work order (largest sizes first); `only` >= 0
+// Tiles of same-size frames in work order (largest sizes first); `only` >= 0
 // restricts the list to one size (the tuner).
 struct WorkList {
   std::vector<int4> tiles;
-  std::vector<long long> pcm_off, out_off;
+  std::vector<int2> jobs;
 };
 
 WorkList build_work(const RaggedPlan& p, int only) {
   WorkList w;
-  std::vector<std::vector<int>> by(ragged_max_log());
-  for (size_t i = 0; i < p.logm.size(); ++i) by[p.logm[i]].push_back((int)i);
+  std::vector<std::vector<int2>> by(ragged_max_log());
+  for (size_t i = 0; i < p.logm.size(); ++i)
+    for (long long f = 0; f < p.frames[i]; ++f) by[p.logm[i]].push_back(make_int2((int)i, (int)f));
   for (int L = ragged_max_log() - 1; L >= 0; --L) {
     if (by[L].empty() || (only >= 0 && L != only)) continue;
-    const bool large = ragged_large_log(L);
-    const int per = large ? 1 : std::max(1, 256 / std::max(1, (1 << L) >> p.lr[L]));
+    const bool whole = ragged_block_log(L) != 0;
+    const int T = std::max(1, (1 << L) >> p.lr[L]);
+    const int per = whole ? 1 : std::max(1, ragged_block_threads() / T);
     for (size_t s = 0; s < by[L].size(); s += per) {
       const int n = (int)std::min<size_t>(per, by[L].size() - s);
-      w.tiles.push_back(make_int4((int)w.pcm_off.size(), n, L, large ? 0 : p.lr[L]));
-      for (int k = 0; k < n; ++k) {
-        const int i = by[L][s + k];
-        w.pcm_off.push_back(p.in_off[i]);
-        w.out_off.push_back(p.out_off[i]);
-      }
+      const int lr = (L == ragged_max_log() - 1) ? 0 : p.lr[L];
+      w.tiles.push_back(make_int4((int)w.jobs.size(), n, L, lr));
+      for (int k = 0; k < n; ++k) w.jobs.push_back(by[L][s + k]);
     }
   }
   return w;
 }
 
 void upload(RaggedPlan& p, const WorkList& w) {
-  RG_CHECK(cudaMemcpyAsync(p.d_pcm_off.get(w.pcm_off.size() * 8), w.pcm_off.data(), w.pcm_off.size() * 8,
-                           cudaMemcpyHostToDevice, p.stream));
-  RG_CHECK(cudaMemcpyAsync(p.d_out_off.get(w.out_off.size() * 8), w.out_off.data(), w.out_off.size() * 8,
-                           cudaMemcpyHostToDevice, p.stream));
-  RG_CHECK(cudaMemcpyAsync(p.d_tiles.get(w.tiles.size() * sizeof(int4)), w.tiles.data(),
+  RG_CHECK(cudaMemcpyAsync(p.d_jobs.get(std::max<size_t>(1, w.jobs.size()) * sizeof(int2)), w.jobs.data(),
+                           w.jobs.size() * sizeof(int2), cudaMemcpyHostToDevice, p.stream));
+  RG_CHECK(cudaMemcpyAsync(p.d_tiles.get(std::max<size_t>(1, w.tiles.size()) * sizeof(int4)), w.tiles.data(),
                            w.tiles.size() * sizeof(int4), cudaMemcpyHostToDevice, p.stream));
   RG_CHECK(cudaStreamSynchronize(p.stream));
   p.ntiles = (int)w.tiles.size();
@@ -128,20 +128,23 @@ RaggedArgs args_for(RaggedPlan& p, const float* pcm, float* re, float* im, float
   a.out_re = re;
   a.out_im = im;
   a.out_mag = mag;
-  a.pcm_off = static_cast<const long long*>(p.d_pcm_off.p);
-  a.out_off = static_cast<const long long*>(p.d_out_off.p);
+  a.items = static_cast<const RaggedItem*>(p.d_items.p);
+  a.jobs = static_cast<const int2*>(p.d_jobs.p);
   a.tiles = static_cast<const int4*>(p.d_tiles.p);
   a.ntiles = p.ntiles;
   a.counter = static_cast<int*>(p.d_counter.p);
   a.scratch = static_cast<float2*>(p.d_scratch.p);
+  a.windows = static_cast<const float*>(p.d_windows.p);
   a.pf = p.pf;
   return a;
 }
 
 // ---------------------------------------------------------------- autotuner
-// Cache of measured choices, keyed by (N, items of that N, transform):
+// Cache of measured choices, keyed by (N, frames of that N, transform and
+// kernel generation):
 // FFTFREE_TUNE_CACHE names the file (default ~/.cache/fftfree_b200/tune.txt);
 // FFTFREE_TUNE=0 turns tuning off (the default schedule of the size).
+const char* const kTuneKind = "r2c.b1024";  // R2C on the 1024-thread persistent kernel
 std::mutex g_cache_mu;
 std::map<std::tuple<long long, long long, std::string>, int> g_cache;
 bool g_cache_loaded = false;
@@ -208,7 +211,7 @@ float time_launch(RaggedPlan& p, const RaggedArgs& a) {
 
 void tune(RaggedPlan& p) {
   std::vector<long long> count(ragged_max_log(), 0);
-  for (int L : p.logm) ++count[L];
+  for (size_t i = 0; i < p.logm.size(); ++i) count[p.logm[i]] += p.frames[i];
   std::lock_guard<std::mutex> lk(g_cache_mu);
   cache_load();
   for (int L = 0; L < ragged_max_log(); ++L) {
@@ -221,7 +224,7 @@ void tune(RaggedPlan& p) {
     p.lr[L] = def;
     if (nc == 1 || !tuning_on()) continue;
     const long long n = 2LL << L;
-    auto it = g_cache.find({n, count[L], "r2c"});
+    auto it = g_cache.find({n, count[L], kTuneKind});
     if (it != g_cache.end() && std::find(cand, cand + nc, it->second) != cand + nc) {
       p.lr[L] = it->second;
       continue;
@@ -240,7 +243,7 @@ void tune(RaggedPlan& p) {
       }
     }
     p.lr[L] = pick;
-    cache_store(n, count[L], "r2c", pick);
+    cache_store(n, count[L], kTuneKind, pick);
   }
 }
 
@@ -288,30 +291,61 @@ using namespace ffb;
 
 extern "C" {
 
-FFT_CFFI_API void* fftfree_ragged_plan(const size_t* sizes, size_t count, int reduce_magnitude,
-                                       int store_polar) {
-  if (!sizes || count == 0 || count > (size_t)1 << 30) return nullptr;
+FFT_CFFI_API void* fftfree_ragged_plan_stft(const size_t* n, const size_t* lengths, const int* window,
+                                            const int* hop, const int* window_kind, const float* window_param,
+                                            size_t count, int reduce_magnitude, int store_polar) {
+  if (!n || !lengths || count == 0 || count > (size_t)1 << 30) return nullptr;
   RaggedPlan* p = nullptr;
   try {
     p = new RaggedPlan();
     RG_CHECK(cudaGetDevice(&p->device));
     p->logm.resize(count);
-    p->in_off.resize(count);
-    p->out_off.resize(count);
+    p->items.resize(count);
+    p->frames.resize(count);
+    std::map<std::tuple<int, int, float>, int> taps;  // (kind, W, p1) -> offset in windows
+    size_t jobs = 0;
     for (size_t i = 0; i < count; ++i) {
-      const int lg = log2_exact(sizes[i]);
-      if (lg < 2 || lg > ragged_max_log()) {
-        std::fprintf(stderr, "[fftfree_b200] fftfree_ragged_plan: size %zu of item %zu is not a power of two "
-                             "in [4, %d]\n", sizes[i], i, 1 << ragged_max_log());
+      const int lg = log2_exact(n[i]);
+      const int N = (int)n[i];
+      const int W = (window && window[i] > 0) ? window[i] : N;
+      const int H = (hop && hop[i] > 0) ? hop[i] : W;
+      if (lg < 2 || lg > ragged_max_log() || W > N || H <= 0 || lengths[i] > ((size_t)1 << 40)) {
+        std::fprintf(stderr, "[fftfree_b200] fftfree_ragged_plan: item %zu: n = %zu must be a power of two in "
+                             "[4, %d], window <= n, hop > 0\n", i, n[i], 1 << ragged_max_log());
         delete p;
         return nullptr;
       }
+      RaggedItem& it = p->items[i];
+      it.pcm_off = (long long)p->samples;
+      it.pcm_len = (long long)lengths[i];
+      it.out_off = (long long)p->bins;
+      it.W = W;
+      it.H = H;
+      it.win_off = -1;
+      const int kind = window_kind ? window_kind[i] : 0;
+      const float p1 = window_param ? window_param[i] : 0.f;
+      if (kind != FFT_WINDOW_RECT) {
+        auto key = std::make_tuple(kind, W, p1);
+        auto f = taps.find(key);
+        if (f == taps.end()) {
+          // taps 4-float aligned, so the 8-byte loads of a frame stay aligned
+          while (p->windows.size() % 4) p->windows.push_back(0.f);
+          const std::vector<float> w = window_taps(kind, W, p1, 0.f, FFT_WINDOW_NORM_NONE);
+          f = taps.emplace(key, (int)p->windows.size()).first;
+          p->windows.insert(p->windows.end(), w.begin(), w.end());
+        }
+        it.win_off = f->second;
+      }
+      // frames of fft_execute_batched with pad_mode 1 (fft_cffi.cpp:710-750)
+      long long fr = 0;
+      if (lengths[i] > 0) fr = (lengths[i] < (size_t)W) ? 1 : 1 + (long long)((lengths[i] - W) / H);
       p->logm[i] = lg - 1;
-      p->in_off[i] = (long long)p->samples;
-      p->out_off[i] = (long long)p->bins;
-      p->samples += sizes[i];
-      p->bins += sizes[i] / 2 + 1;
+      p->frames[i] = fr;
+      p->samples += lengths[i];
+      p->bins += (size_t)fr * (n[i] / 2 + 1);
+      jobs += (size_t)fr;
     }
+    if (jobs > (size_t)0x7fffffff) throw std::runtime_error("too many frames");
     p->pf.r2c_half = 1;
     p->pf.polar = store_polar ? 1 : 0;
     p->pf.reduce = (!store_polar && reduce_magnitude) ? 1 : 0;
@@ -321,14 +355,20 @@ FFT_CFFI_API void* fftfree_ragged_plan(const size_t* sizes, size_t count, int re
     if (!twiddle_pass_tables(p->stream)) throw std::runtime_error("twiddle tables");
     p->grid = ragged_grid();
     p->d_counter.get(sizeof(int));
-    bool any_large = false;
-    for (int L : p->logm) any_large = any_large || ragged_large_log(L);
-    if (any_large) p->d_scratch.get((size_t)p->grid * ragged_scratch_per_block());
+    RG_CHECK(cudaMemcpyAsync(p->d_items.get(count * sizeof(RaggedItem)), p->items.data(),
+                             count * sizeof(RaggedItem), cudaMemcpyHostToDevice, p->stream));
+    if (!p->windows.empty())
+      RG_CHECK(cudaMemcpyAsync(p->d_windows.get(p->windows.size() * 4), p->windows.data(), p->windows.size() * 4,
+                               cudaMemcpyHostToDevice, p->stream));
+    bool any_split = false;
+    for (size_t i = 0; i < count; ++i) any_split = any_split || (p->logm[i] == ragged_max_log() - 1 && p->frames[i]);
+    if (any_split) p->d_scratch.get((size_t)p->grid * ragged_scratch_per_block());
     // staging (host buffers) and the tuner's buffers
-    RG_CHECK(cudaMemsetAsync(p->d_in.get(p->samples * 4), 0, p->samples * 4, p->stream));
-    p->d_re.get(p->bins * 4);
-    p->d_im.get(p->bins * 4);
-    p->d_mag.get(p->bins * 4);
+    RG_CHECK(cudaMemsetAsync(p->d_in.get(std::max<size_t>(1, p->samples) * 4), 0,
+                             std::max<size_t>(1, p->samples) * 4, p->stream));
+    p->d_re.get(std::max<size_t>(1, p->bins) * 4);
+    p->d_im.get(std::max<size_t>(1, p->bins) * 4);
+    p->d_mag.get(std::max<size_t>(1, p->bins) * 4);
     tune(*p);
     upload(*p, build_work(*p, -1));
     return p;
@@ -336,6 +376,18 @@ FFT_CFFI_API void* fftfree_ragged_plan(const size_t* sizes, size_t count, int re
     delete p;
     return nullptr;
   }
+}
+
+FFT_CFFI_API void* fftfree_ragged_plan(const size_t* sizes, size_t count, int reduce_magnitude,
+                                       int store_polar) {
+  // one frame per item: window = hop = the item's size, no window taps
+  return fftfree_ragged_plan_stft(sizes, sizes, nullptr, nullptr, nullptr, nullptr, count, reduce_magnitude,
+                                  store_polar);
+}
+
+FFT_CFFI_API size_t fftfree_ragged_frames(void* plan, size_t item) {
+  RaggedPlan* p = as_plan(plan);
+  return (p && item < p->frames.size()) ? (size_t)p->frames[item] : 0;
 }
 
 FFT_CFFI_API size_t fftfree_ragged_samples(void* plan) {
@@ -352,7 +404,7 @@ FFT_CFFI_API int fftfree_ragged_schedule(void* plan, size_t n) {
   RaggedPlan* p = as_plan(plan);
   const int lg = log2_exact(n);
   if (!p || lg < 2 || lg > ragged_max_log()) return 0;
-  return ragged_large_log(lg - 1) ? 0 : (1 << p->lr[lg - 1]);
+  return (lg - 1 == ragged_max_log() - 1) ? 0 : (1 << p->lr[lg - 1]);
 }
 
 FFT_CFFI_API void fftfree_ragged_set_stream(void* plan, void* stream) {

@@ -181,11 +181,27 @@ FFT_CFFI_API size_t fftfree_stft_magnitude_backward_phasor(void* handle, const f
  * size or a CUDA failure. */
 FFT_CFFI_API void* fftfree_ragged_plan(const size_t* sizes, size_t count, int reduce_magnitude,
                                        int store_polar);
+/* The same for ragged mixes of size AND framing: item i is a real signal of
+ * lengths[i] samples framed as fft_execute_batched frames it with pad_mode 1
+ * on a context (n[i], window[i], hop[i], transform = R2C, half_spectrum = 1,
+ * apply_windows with analysis window kind window_kind[i] and parameter
+ * window_param[i], norm policy 0) (fft_cffi.cpp:701-824, 163-208): frames of
+ * window[i] <= n[i] samples every hop[i] samples, zero-padded to n[i]
+ * (powers of two, 4 .. 65536), a lone partial frame when the signal is
+ * shorter than one.  Its frames' planar rows of n[i]/2 + 1 bins are packed
+ * frame after frame, items in order.  window, hop, window_kind and
+ * window_param may be NULL (window = hop = n, rectangular); window[i] or
+ * hop[i] of 0 means n[i] (hop: window[i]). */
+FFT_CFFI_API void* fftfree_ragged_plan_stft(const size_t* n, const size_t* lengths, const int* window,
+                                            const int* hop, const int* window_kind, const float* window_param,
+                                            size_t count, int reduce_magnitude, int store_polar);
+/* Frames the plan computes for item i (0 for a bad index). */
+FFT_CFFI_API size_t fftfree_ragged_frames(void* plan, size_t item);
 /* Total input samples / output bins per array of a plan (0 for NULL). */
 FFT_CFFI_API size_t fftfree_ragged_samples(void* plan);
 FFT_CFFI_API size_t fftfree_ragged_bins(void* plan);
 /* The pass radix the plan runs for size n (0: n is absent from the plan's
- * single-pass sizes, or takes the three-phase path). */
+ * single-pass sizes, or takes the two-half path of 65536 points). */
 FFT_CFFI_API int fftfree_ragged_schedule(void* plan, size_t n);
 /* Stream of the plan's launches (NULL: the plan's own stream). */
 FFT_CFFI_API void fftfree_ragged_set_stream(void* plan, void* cuda_stream);
