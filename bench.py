@@ -198,6 +198,9 @@ CASES = {
     "c2c_n65536_b512": "C2C N=65536 x 512 complex64, four-step (two passes)",
     "ragged_4096": "ragged batch: 4096 R2C signals, N = 2^e, e uniform in 6..16 (seed 2), one persistent launch",
     "fft2d_4096x4096_b4": "2-D C2C of 4 column-major 4096 x 4096 complex64 matrices (column pass + strided row pass)",
+    "r2c_n4096_polar_b8192": "R2C N=W=H=4096, half spectrum, store_polar, 8192 frames (fft_execute_batched)",
+    "c2r_n4096_polar_b8192": "C2R N=4096 half spectrum polar input (Cooley-Tukey pre-hook), 8192 frames "
+                             "(fft_execute_complex_batched)",
 }
 
 
@@ -241,6 +244,23 @@ def run_case(args):
         plan.set_stream(stream.cuda_stream)
         re, im, mg = (torch.empty(plan.bins, device="cuda") for _ in range(3))
         fn, nbytes = (lambda: plan.execute(pcm, re, im, mg)), plan.samples * 4 + 3 * plan.bins * 4
+    elif name in ("r2c_n4096_polar_b8192", "c2r_n4096_polar_b8192"):
+        B, N = 8192, 4096
+        bins = N // 2 + 1
+        pcm = torch.rand(B * N, device="cuda", generator=g) * 2 - 1
+        re, im, mg = (torch.empty(B * bins, device="cuda") for _ in range(3))
+        c = ff.FftContext.full_v2(N, kernel=2, window=N, hop=N, transform=1, half_spectrum=1, store_polar=1)
+        c.set_stream(stream.cuda_stream)
+        c.set_async(True)
+        c.execute_batched(pcm, re, im, mg, pcm_len=B * N)
+        if name.startswith("r2c"):
+            fn, nbytes = (lambda: c.execute_batched(pcm, re, im, mg, pcm_len=B * N)), B * N * 4 + 3 * B * bins * 4
+        else:
+            ci = ff.FftContext.full_v2(N, kernel=0, inverse=1, transform=2, half_spectrum=1, store_polar=1)
+            ci.set_stream(stream.cuda_stream)
+            ci.set_async(True)
+            out = torch.empty(B * N, device="cuda")
+            fn, nbytes = (lambda: ci.execute_complex_batched(re, im, B, out)), 2 * B * bins * 4 + B * N * 4
     elif name == "stft_n1024_h256":
         L = 128 * 65536
         pcm = torch.rand(L, device="cuda", generator=g) * 2 - 1
@@ -621,7 +641,9 @@ def measure_autograd(torch, stream, timed):
     noise, seed 4), Hann W = N = 2048, H = 512 (509 frames x 1025 bins).
     Plain forward = the magnitude STFT kernel alone; fwd+bwd = the
     torch.autograd.Function forward and backward for a given upstream
-    gradient; with_loss adds sum((|X| - T)^2) and its torch elementwise ops."""
+    gradient; with_loss adds sum((|X| - T)^2) and its torch elementwise ops;
+    loss_fused is the same loss through stft_magnitude_l2_loss (one fused
+    forward kernel, one scaled adjoint kernel)."""
     from fftfree_b200 import autograd as ag
 
     S, L, N, H = 64, 262144, 2048, 512
@@ -652,10 +674,17 @@ def measure_autograd(torch, stream, timed):
         xr.grad = None
         (ag.stft_magnitude(xr, plan) - target).square().sum().backward()
 
+    def with_loss_fused():
+        xr.grad = None
+        ag.stft_magnitude_l2_loss(xr, target, plan).backward()
+
     # saved phasor (the default at this size): fwd writes |X| and X / |X|, bwd reads g and X / |X|
     assert plan.stores_phase(xr)
     fb = timed(fwd_bwd, in_b + 3 * mag_b + 3 * mag_b + in_b)
     fl = timed(with_loss, in_b + 3 * mag_b + 3 * mag_b + in_b)
+    # fused loss: fwd reads x and T, writes the residual and the phasor; bwd
+    # reads them and writes dL/dx
+    flf = timed(with_loss_fused, in_b + 4 * mag_b + 3 * mag_b + in_b)
     _, ph = plan.magnitude_phasor(x)
     bwd_ph = timed(lambda: plan.magnitude_backward_phasor(ph, upstream, L), 3 * mag_b + in_b)
     plan.close()
@@ -666,9 +695,10 @@ def measure_autograd(torch, stream, timed):
     plan.close()
     return {"signals": S, "samples": L, "n_fft": N, "hop": H, "frames": F, "bins": bins,
             "fwd": fwd, "bwd_recompute": bwd, "bwd_saved_phasor": bwd_ph, "fwd_bwd": fb,
-            "fwd_bwd_with_loss": fl, "fwd_bwd_recompute": fb_rc,
+            "fwd_bwd_with_loss": fl, "fwd_bwd_loss_fused": flf, "fwd_bwd_recompute": fb_rc,
             "ratio_fwd_bwd_over_fwd": round(fb["ms"] / fwd["ms"], 3),
             "ratio_with_loss_over_fwd": round(fl["ms"] / fwd["ms"], 3),
+            "ratio_loss_fused_over_fwd": round(flf["ms"] / fwd["ms"], 3),
             "ratio_recompute_over_fwd": round(fb_rc["ms"] / fwd["ms"], 3),
             "frames_per_s_fwd": round(S * F / (fwd["ms"] * 1e-3), 1)}
 

@@ -116,6 +116,12 @@ _SIGS = [
                                                        ctypes.c_size_t, c_float_p, c_float_p, ctypes.c_size_t]),
     ("fftfree_stft_magnitude_backward_phasor", ctypes.c_size_t, [ctypes.c_void_p, c_float_p, ctypes.c_size_t,
                                                                 ctypes.c_size_t, c_float_p, c_float_p]),
+    ("fftfree_stft_l2_partials", ctypes.c_size_t, [ctypes.c_void_p, ctypes.c_size_t]),
+    ("fftfree_stft_magnitude_l2", ctypes.c_size_t, [ctypes.c_void_p, c_float_p, ctypes.c_size_t, ctypes.c_size_t,
+                                                    c_float_p, c_float_p, c_float_p, c_float_p, ctypes.c_size_t]),
+    ("fftfree_stft_magnitude_backward_phasor_scaled", ctypes.c_size_t,
+     [ctypes.c_void_p, c_float_p, ctypes.c_size_t, ctypes.c_size_t, c_float_p, c_float_p, c_float_p,
+      ctypes.c_float]),
     ("fftfree_ragged_plan", ctypes.c_void_p, [ctypes.POINTER(ctypes.c_size_t), ctypes.c_size_t, ctypes.c_int,
                                               ctypes.c_int]),
     ("fftfree_ragged_plan_stft", ctypes.c_void_p, [ctypes.POINTER(ctypes.c_size_t), ctypes.POINTER(ctypes.c_size_t),
@@ -317,6 +323,21 @@ class FftContext:
     def stft_magnitude_backward_phasor(self, phasor, signals, length, grad_mag, grad_pcm) -> int:
         return int(lib().fftfree_stft_magnitude_backward_phasor(self.handle, _fp(phasor), signals, length,
                                                                 _fp(grad_mag), _fp(grad_pcm)))
+
+    def stft_l2_partials(self, frames_total) -> int:
+        return int(lib().fftfree_stft_l2_partials(self.handle, frames_total))
+
+    def stft_magnitude_l2(self, pcm, signals, length, target, out_residual, out_phasor, out_partials,
+                          max_frames=0) -> int:
+        return int(lib().fftfree_stft_magnitude_l2(self.handle, _fp(pcm), signals, length, _fp(target),
+                                                   _fp(out_residual), _fp(out_phasor), _fp(out_partials),
+                                                   max_frames))
+
+    def stft_magnitude_backward_phasor_scaled(self, phasor, signals, length, grad_mag, grad_pcm, scale=None,
+                                              factor=1.0) -> int:
+        return int(lib().fftfree_stft_magnitude_backward_phasor_scaled(self.handle, _fp(phasor), signals, length,
+                                                                       _fp(grad_mag), _fp(grad_pcm), _fp(scale),
+                                                                       float(factor)))
 
     def stft_magnitude_backward(self, pcm, signals, length, grad_mag, grad_pcm) -> int:
         return int(lib().fftfree_stft_magnitude_backward(self.handle, _fp(pcm), signals, length, _fp(grad_mag),

@@ -145,6 +145,48 @@ class StftPlan:
             raise RuntimeError(f"fftfree_stft_magnitude_backward_phasor returned {got} frames, expected {F}")
         return gx[0] if ph.dim() == 2 else gx
 
+    def magnitude_l2(self, x: torch.Tensor, target: torch.Tensor):
+        """One pass for the spectral L2 loss: (partial sums of (|X| - T)^2,
+        residual |X| - T, unit phasor), the residual and phasor in the layout
+        of ``magnitude``; the loss is the sum of the partial sums."""
+        x = self._check(x)
+        x2 = x.view(1, -1) if x.dim() == 1 else x
+        S, L = x2.shape
+        F = self.frames(L)
+        if F == 0:
+            raise ValueError("signal shorter than one frame")
+        tg = target.to(device=x.device, dtype=torch.float32).contiguous()
+        if tg.numel() != S * F * self.bins:
+            raise ValueError("target does not match the magnitude STFT's shape")
+        res = torch.empty((S, F, self.bins), dtype=torch.float32, device=x.device)
+        ph = torch.empty((S, F, self.bins), dtype=torch.complex64, device=x.device)
+        parts = torch.empty(self.ctx.stft_l2_partials(S * F), dtype=torch.float32, device=x.device)
+        self._bind_stream()
+        got = self.ctx.stft_magnitude_l2(x2, S, L, tg, res, ph, parts)
+        if got != F:
+            raise RuntimeError(f"fftfree_stft_magnitude_l2 returned {got} frames, expected {F}")
+        return parts, res, ph
+
+    def magnitude_backward_phasor_scaled(self, phasor: torch.Tensor, grad_mag: torch.Tensor, length: int,
+                                         scale: Optional[torch.Tensor], factor: float) -> torch.Tensor:
+        """``magnitude_backward_phasor`` times factor (times the one-element
+        CUDA tensor ``scale``, read by the kernel)."""
+        ph = phasor.contiguous()
+        S = 1 if ph.dim() == 2 else ph.shape[0]
+        F = self.frames(length)
+        g = grad_mag.to(dtype=torch.float32).contiguous()
+        if ph.numel() != S * F * self.bins or g.numel() != ph.numel():
+            raise ValueError("phasor / grad_mag do not match the forward output")
+        sc = None
+        if scale is not None:
+            sc = scale.to(device=ph.device, dtype=torch.float32).reshape(1).contiguous()
+        gx = torch.empty((S, length), dtype=torch.float32, device=ph.device)
+        self._bind_stream()
+        got = self.ctx.stft_magnitude_backward_phasor_scaled(ph, S, length, g, gx, sc, factor)
+        if got != F:
+            raise RuntimeError(f"fftfree_stft_magnitude_backward_phasor_scaled returned {got} frames, expected {F}")
+        return gx[0] if ph.dim() == 2 else gx
+
     def magnitude_backward(self, x: torch.Tensor, grad_mag: torch.Tensor) -> torch.Tensor:
         """d(sum(grad_mag * |STFT x|))/dx, shaped like x."""
         x = self._check(x)
@@ -192,6 +234,43 @@ class _StftMagnitude(torch.autograd.Function):
 def stft_magnitude(x: torch.Tensor, plan: StftPlan) -> torch.Tensor:
     """Differentiable |STFT x| through the library's kernels."""
     return _StftMagnitude.apply(x, plan)
+
+
+class _StftMagnitudeL2(torch.autograd.Function):
+    @staticmethod
+    def forward(ctx, x: torch.Tensor, target: torch.Tensor, plan: StftPlan) -> torch.Tensor:
+        parts, res, ph = plan.magnitude_l2(x, target)
+        ctx.plan = plan
+        ctx.length = x.shape[-1]
+        ctx.x_dim = x.dim()
+        ctx.save_for_backward(ph, res)
+        return parts.sum()
+
+    @staticmethod
+    def backward(ctx, grad_out: torch.Tensor):
+        ph, res = ctx.saved_tensors
+        gx = None
+        if ctx.needs_input_grad[0]:
+            gx = ctx.plan.magnitude_backward_phasor_scaled(ph, res, ctx.length, grad_out, 2.0)
+            if ctx.x_dim == 1:
+                gx = gx.reshape(-1)
+        gt = None
+        if ctx.needs_input_grad[1]:
+            gt = res * (-2.0 * grad_out)
+            if ctx.x_dim == 1:
+                gt = gt[0]
+        return gx, gt, None
+
+
+def stft_magnitude_l2_loss(x: torch.Tensor, target: torch.Tensor, plan: StftPlan) -> torch.Tensor:
+    """sum((|STFT x| - target)^2), differentiable, fused: one forward kernel
+    writes the residual, the unit phasor and the loss's partial sums; the
+    backward is one adjoint kernel scaled by the upstream gradient on the
+    device.  Signals whose phasor exceeds the plan's ``phase_budget`` take
+    ``stft_magnitude`` and torch's elementwise ops instead."""
+    if not plan.stores_phase(x):
+        return (stft_magnitude(x, plan) - target).square().sum()
+    return _StftMagnitudeL2.apply(x, target, plan)
 
 
 def spectral_convergence(mag: torch.Tensor, target: torch.Tensor) -> float:

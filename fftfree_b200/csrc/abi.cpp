@@ -271,11 +271,8 @@ static bool single_pass(int N, bool real_input) {
 }
 
 static float2* scratch_for(FftContext* c, int N, long long batch, size_t* chunk) {
-  *chunk = four_step_chunk(ilog2((size_t)N), batch);
-  // two slots when the multi-pass pipeline alternates between chunks,
-  // one when a single chunk covers the batch
-  const size_t slots = ((long long)*chunk < batch) ? 2 : 1;
-  return static_cast<float2*>(c->d_scratch.get(slots * *chunk * (size_t)N * sizeof(float2)));
+  const size_t points = four_step_scratch(ilog2((size_t)N), batch, chunk);
+  return static_cast<float2*>(c->d_scratch.get(points * sizeof(float2)));
 }
 
 static void setup_device(FftContext* c) {
@@ -1211,11 +1208,15 @@ static int mag_grad_run() {
 }
 
 // Shared body of the magnitude STFT entry points; out_phasor (X / |X| as
-// interleaved pairs, 0 where |X| = 0) is written when not null.
+// interleaved pairs, 0 where |X| = 0) is written when not null; with a
+// target, out_mag receives |X| - target and out_partials the squared
+// residuals' partial sums.
 static size_t stft_magnitude(void* handle, const float* pcm, size_t signals, size_t length, float* out_mag,
-                             float* out_phasor, size_t max_frames, const char* who) {
+                             float* out_phasor, size_t max_frames, const char* who, const float* target = nullptr,
+                             float* out_partials = nullptr) {
   FftContext* c = as_ctx(handle);
   if (!c || !pcm || !out_mag || signals == 0 || length == 0) return 0;
+  if (target && (!out_phasor || !out_partials)) return 0;
   try {
     std::lock_guard<std::recursive_mutex> lk(c->mu);
     if (!mag_grad_ctx_ok(c, who)) return 0;
@@ -1229,9 +1230,16 @@ static size_t stft_magnitude(void* handle, const float* pcm, size_t signals, siz
     bool any_host = !is_device_ptr(pcm);
     const float* d_pcm = stage_in(c, c->d_in0, pcm, signals * length);
     OutTarget o = stage_out(c->d_out2, out_mag, outn);
-    OutTarget op;
+    OutTarget op, opart;
     if (out_phasor) op = stage_out(c->d_out1, out_phasor, 2 * outn);
-    any_host = any_host || o.host || op.host;
+    const float* d_tg = nullptr;
+    const long long nparts = stft_loss_parts((long long)(signals * frames), c->N);
+    if (target) {
+      any_host = any_host || !is_device_ptr(target);
+      d_tg = stage_in(c, c->d_in1, target, outn);
+      opart = stage_out(c->d_frames, out_partials, (size_t)nparts);
+    }
+    any_host = any_host || o.host || op.host || opart.host;
     StftArgs a{};
     a.pcm = d_pcm;
     a.pcm_len = (long long)length;
@@ -1247,10 +1255,13 @@ static size_t stft_magnitude(void* handle, const float* pcm, size_t signals, siz
     a.out_phasor = out_phasor ? reinterpret_cast<float2*>(op.dev) : nullptr;
     a.sig_frames = (long long)frames;
     a.sig_stride = (long long)length;
-    a.mag_only = out_phasor ? 2 : 1;
+    a.mag_only = target ? 3 : (out_phasor ? 2 : 1);
+    a.target = d_tg;
+    a.loss_part = target ? opart.dev : nullptr;
     FFB_CHECK(launch_stft(a, c->logr_req, c->stream, &c->launches));
     finish_out(c, o);
     if (out_phasor) finish_out(c, op);
+    if (target) finish_out(c, opart);
     finish_call(c, any_host);
     return frames;
   } catch (...) {
@@ -1270,10 +1281,24 @@ FFT_CFFI_API size_t fftfree_stft_magnitude_phasor(void* handle, const float* pcm
                         "fftfree_stft_magnitude_phasor");
 }
 
+FFT_CFFI_API size_t fftfree_stft_l2_partials(void* handle, size_t frames_total) {
+  FftContext* c = as_ctx(handle);
+  return c ? (size_t)stft_loss_parts((long long)frames_total, c->N) : 0;
+}
+
+FFT_CFFI_API size_t fftfree_stft_magnitude_l2(void* handle, const float* pcm, size_t signals, size_t length,
+                                              const float* target, float* out_residual, float* out_phasor,
+                                              float* out_partials, size_t max_frames) {
+  if (!target || !out_phasor || !out_partials) return 0;
+  return stft_magnitude(handle, pcm, signals, length, out_residual, out_phasor, max_frames,
+                        "fftfree_stft_magnitude_l2", target, out_partials);
+}
+
 // Shared body of the gradient entry points: the spectrum comes from pcm
 // (recomputed) or from a saved unit phasor.
 static size_t stft_magnitude_backward(void* handle, const float* pcm, const float* phasor, size_t signals,
-                                      size_t length, const float* grad_mag, float* grad_pcm, const char* who) {
+                                      size_t length, const float* grad_mag, float* grad_pcm, const char* who,
+                                      const float* scale = nullptr, float factor = 1.0f) {
   FftContext* c = as_ctx(handle);
   if (!c || !(pcm || phasor) || !grad_mag || !grad_pcm || signals == 0 || length == 0) return 0;
   try {
@@ -1314,6 +1339,9 @@ static size_t stft_magnitude_backward(void* handle, const float* pcm, const floa
     a.grad_pcm = o.dev;
     a.span = mag_grad_span(H);
     a.run = mag_grad_run();
+    a.factor = factor;
+    a.scale = scale;
+    if (scale && !is_device_ptr(scale)) throw std::runtime_error("scale must be device memory");
     FFB_CHECK(launch_stft_mag_grad(a, c->logr_req, c->stream, &c->launches));
     finish_out(c, o);
     finish_call(c, any_host);
@@ -1336,6 +1364,15 @@ FFT_CFFI_API size_t fftfree_stft_magnitude_backward_phasor(void* handle, const f
   if (!phasor) return 0;
   return stft_magnitude_backward(handle, nullptr, phasor, signals, length, grad_mag, grad_pcm,
                                  "fftfree_stft_magnitude_backward_phasor");
+}
+
+FFT_CFFI_API size_t fftfree_stft_magnitude_backward_phasor_scaled(void* handle, const float* phasor,
+                                                                  size_t signals, size_t length,
+                                                                  const float* grad_mag, float* grad_pcm,
+                                                                  const float* scale, float factor) {
+  if (!phasor) return 0;
+  return stft_magnitude_backward(handle, nullptr, phasor, signals, length, grad_mag, grad_pcm,
+                                 "fftfree_stft_magnitude_backward_phasor_scaled", scale, factor);
 }
 
 FFT_CFFI_API void fftfree_set_stream(void* handle, void* cuda_stream) {

@@ -186,10 +186,38 @@ __device__ __forceinline__ const float* stft_frame(const float* pcm, long long p
   return pcm + start;
 }
 
+// Slots of squared-residual partial sums per frame of an L2-loss STFT of
+// M = N/2 complex points: one per warp of the widest transform group
+// (T = M / 4 threads), at least one.
+__host__ __device__ constexpr int loss_slots(int M) { return M / 128 > 1 ? M / 128 : 1; }
+
+// Sum of v over the T threads of one transform group, into slots
+// part[0 .. loss_slots(M)) of its frame: one sum per warp (or per group when
+// T < 32), in a fixed order; unused slots are zeroed.  Every thread of the
+// group calls it.
+template <class S>
+__device__ __forceinline__ void group_loss_partial(float v, int t, float* part) {
+  constexpr int T = S::T;
+  constexpr int W = T < 32 ? T : 32;
+  constexpr int P = T / 32 > 1 ? T / 32 : 1;
+  constexpr int SLOTS = loss_slots(S::M);
+  const unsigned lane = threadIdx.x & 31u;
+  const unsigned mask = (W == 32) ? 0xffffffffu : (((1u << W) - 1u) << (lane & ~(unsigned)(W - 1)));
+#pragma unroll
+  for (int o = W / 2; o > 0; o >>= 1) v += __shfl_xor_sync(mask, v, o, W);
+  if ((t & (W - 1)) == 0) part[t / W] = v;
+  if (t == 0) {
+#pragma unroll
+    for (int p = P; p < SLOTS; ++p) part[p] = 0.f;
+  }
+}
+
 // ------------------------------------------------------------------ STFT IO
 // MODE: 0 plain / imag clear, 1 reduce_magnitude, 2 store_polar, 3 |X| only
 // (forward half spectrum, magnitude array alone), 4 |X| into the magnitude
-// array and the unit phasor X / |X| into out_phasor (0 where |X| = 0).
+// array and the unit phasor X / |X| into out_phasor (0 where |X| = 0), 5 the
+// residual |X| - target into the magnitude array, the unit phasor, and the
+// frame's sum of squared residuals (loss_part, loss_slots per frame).
 template <int MODE>
 struct StftIO {
   StftArgs a;
@@ -295,7 +323,7 @@ struct StftIO {
     GroupSync::sync<S>();
     if (f >= a.frames) return;
     const long long ob = f * a.out_stride;
-    float* re = (MODE == 4) ? reinterpret_cast<float*>(a.out_phasor + ob) : a.out_re + (MODE == 3 ? 0 : ob);
+    float* re = (MODE >= 4) ? reinterpret_cast<float*>(a.out_phasor + ob) : a.out_re + (MODE == 3 ? 0 : ob);
     float* im = a.out_im + (MODE >= 3 ? 0 : ob);
     float* mg = a.out_mag + ob;
     const bool mag_is_re = (MODE == 1) || (MODE == 2 && a.mag_from_real);
@@ -313,6 +341,31 @@ struct StftIO {
       float* pr = re + t;
       float* pi = im + t;
       float* pm = mg + t;
+      if constexpr (MODE == 5) {
+        const float* tg = a.target + ob + t;
+        float2* ph = reinterpret_cast<float2*>(re) + t;
+        float acc = 0.f;
+#pragma unroll
+        for (int i = 0; i < R; ++i) {
+          const float2 zm = sm[pidx((M - t - i * T) & (M - 1))];
+          float2 X = untangle_bin(v[i], zm, w.half(i));
+          if (i == 0 && t == 0) X.y = 0.f;  // DC
+          float m;
+          ph[i * T] = mag_phasor(X, &m);
+          const float r = m - __ldg(tg + i * T);
+          pm[i * T] = r;
+          acc = __fmaf_rn(r, r, acc);
+        }
+        if (t == 0) {  // Nyquist X[M] = Re Z[0] - Im Z[0]
+          float m;
+          reinterpret_cast<float2*>(re)[M] = mag_phasor(make_float2(v[0].x - v[0].y, 0.f), &m);
+          const float r = m - __ldg(a.target + ob + M);
+          mg[M] = r;
+          acc = __fmaf_rn(r, r, acc);
+        }
+        group_loss_partial<S>(acc, t, a.loss_part + f * loss_slots(M));
+        return;
+      }
 #pragma unroll
       for (int i = 0; i < R; ++i) {
         const float2 zm = sm[pidx((M - t - i * T) & (M - 1))];

@@ -96,6 +96,12 @@ __device__ __forceinline__ void grad_load(const MagGradArgs& a, const float* pcm
   }
 }
 
+// The upstream gradient's factor: a.factor, times the device scalar a.scale
+// when set (a loss's upstream gradient, read here rather than on the host).
+__device__ __forceinline__ float grad_scale(const MagGradArgs& a) {
+  return a.scale ? a.factor * __ldg(a.scale) : a.factor;
+}
+
 // dL/dX scaled onto the Hermitian half spectrum: V = g X / |X|, 0 at |X| = 0.
 __device__ __forceinline__ float2 mag_chain(float2 X, float g) {
   const float m = cabs_fast(X.x, X.y);
@@ -177,9 +183,10 @@ __device__ __forceinline__ void frame_grad(const MagGradArgs& a, const float* pc
   grad_load<S>(a, pcm, f, ok, t, v, &cnt);
   // upstream gradient of this frame's bins, fetched before the transform
   const float* gf = gsig + (ok ? f : 0) * (long long)(M + 1);
+  const float sc = grad_scale(a);
   float gk[R];
 #pragma unroll
-  for (int i = 0; i < R; ++i) gk[i] = ok ? __ldg(gf + t + i * T) : 0.f;
+  for (int i = 0; i < R; ++i) gk[i] = ok ? sc * __ldg(gf + t + i * T) : 0.f;
   fft_engine<S, GroupSync>(v, t, sm, tw);
 
   // Untangle Z (the M-point transform of z) into X[k], k = t + i*T, and
@@ -203,7 +210,7 @@ __device__ __forceinline__ void frame_grad(const MagGradArgs& a, const float* pc
   float2 ynyq = make_float2(0.f, 0.f);
   if (t == 0) {  // Nyquist X[M] = Re Z[0] - Im Z[0]
     const float xn = v[0].x - v[0].y;
-    const float gn = ok ? __ldg(gf + M) : 0.f;
+    const float gn = ok ? sc * __ldg(gf + M) : 0.f;
     ynyq = make_float2(2.f * mag_chain(make_float2(xn, 0.f), gn).x, 0.f);
   }
   GroupSync::sync<S>();  // every read of Z is done
@@ -223,16 +230,17 @@ __device__ __forceinline__ void frame_grad_phasor(const MagGradArgs& a, const fl
     if (cnt > a.W) cnt = a.W;
   }
   const long long off = (ok ? f : 0) * (long long)(M + 1);
+  const float sc = grad_scale(a);
   float2 y[R];
 #pragma unroll
   for (int i = 0; i < R; ++i) {
     const int k = t + i * T;
     float2 V = make_float2(0.f, 0.f);
-    if (ok) V = cscale(__ldg(usig + off + k), __ldg(gsig + off + k));
+    if (ok) V = cscale(__ldg(usig + off + k), sc * __ldg(gsig + off + k));
     y[i] = (i == 0 && t == 0) ? make_float2(2.f * V.x, 0.f) : V;  // DC is real
   }
   float2 ynyq = make_float2(0.f, 0.f);
-  if (t == 0 && ok) ynyq = make_float2(2.f * __ldg(gsig + off + M) * __ldg(usig + off + M).x, 0.f);  // Nyquist
+  if (t == 0 && ok) ynyq = make_float2(2.f * sc * __ldg(gsig + off + M) * __ldg(usig + off + M).x, 0.f);  // Nyquist
   grad_inverse<S>(a, y, ynyq, cnt, t, sm, tw, v);
 }
 

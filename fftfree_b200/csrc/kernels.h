@@ -38,10 +38,16 @@ struct StftArgs {
   long long sig_frames;
   long long sig_stride;
   // forward R2C half spectrum, bins 0..N/2: 1 = only |X| (out_mag),
-  // 2 = |X| (out_mag) and the unit phasor X / |X| (out_phasor, 0 where |X| = 0)
+  // 2 = |X| (out_mag) and the unit phasor X / |X| (out_phasor, 0 where |X| = 0),
+  // 3 = the residual |X| - target (out_mag), the phasor, and per-warp sums of
+  // the squared residuals (loss_part)
   int mag_only;
   float2* out_phasor;
+  const float* target;  // mag_only 3: same layout as out_mag
+  float* loss_part;     // mag_only 3: stft_loss_parts(frames, N) floats
 };
+// Partial sums of the squared residual an L2-loss launch writes.
+long long stft_loss_parts(long long frames, int N);
 
 // Gradient of the magnitude STFT (forward R2C half spectrum, |X| per bin)
 // with respect to the signals: recomputes each frame's spectrum, applies
@@ -60,6 +66,10 @@ struct MagGradArgs {
   float* grad_pcm;        // signals x sig_stride; every sample < pcm_len written
   int span;               // general form: samples of one signal owned by one block
   int run;                // sliding form: frames of one signal per thread group (0: general form only)
+  // the gradient is scaled by factor (times *scale when not null, a device
+  // scalar: the upstream gradient of a loss, read without a host sync)
+  float factor;
+  const float* scale;
 };
 
 // Complex columns in/out with the plan hooks (C++ fft_inplace_batched).
@@ -216,6 +226,9 @@ cudaError_t launch_ragged(const RaggedArgs& a, int grid, cudaStream_t s, uint64_
 // that stays resident in L2).
 int max_multi_pass_log();
 size_t four_step_chunk(int log_n, long long batch);
+// Complex points of scratch a multi-pass call over `batch` transforms of
+// 2^log_n points needs, and the `chunk` to pass to the launchers.
+size_t four_step_scratch(int log_n, long long batch, size_t* chunk);
 cudaError_t launch_four_step_stft(const StftArgs& a, float2* scratch, size_t chunk, cudaStream_t s,
                                   uint64_t* launches);
 cudaError_t launch_four_step_c2c(const C2cArgs& a, float2* scratch, size_t chunk, cudaStream_t s,

@@ -164,6 +164,28 @@ FFT_CFFI_API size_t fftfree_stft_magnitude_backward_phasor(void* handle, const f
                                                            size_t length, const float* grad_mag,
                                                            float* grad_pcm);
 
+/* The spectral L2 loss sum((|X| - target)^2) in one pass: |X| - target into
+ * out_residual (target and residual with the layout of
+ * fftfree_stft_magnitude's output), the unit phasor into out_phasor, and the
+ * squared residuals summed per frame into fftfree_stft_l2_partials(handle,
+ * signals * frames) partial sums in out_partials (their sum is the loss; a
+ * fixed summation order, no atomics).  Its gradient is
+ * fftfree_stft_magnitude_backward_phasor_scaled(phasor, grad_mag = residual,
+ * scale = the loss's upstream gradient, factor = 2).  Returns the frames per
+ * signal, 0 on failure. */
+FFT_CFFI_API size_t fftfree_stft_l2_partials(void* handle, size_t frames_total);
+FFT_CFFI_API size_t fftfree_stft_magnitude_l2(void* handle, const float* pcm, size_t signals, size_t length,
+                                              const float* target, float* out_residual, float* out_phasor,
+                                              float* out_partials, size_t max_frames);
+
+/* fftfree_stft_magnitude_backward_phasor with the gradient scaled by factor,
+ * times *scale when scale is not NULL (a device pointer to one float, read by
+ * the kernel: an upstream gradient that never visits the host). */
+FFT_CFFI_API size_t fftfree_stft_magnitude_backward_phasor_scaled(void* handle, const float* phasor,
+                                                                  size_t signals, size_t length,
+                                                                  const float* grad_mag, float* grad_pcm,
+                                                                  const float* scale, float factor);
+
 /* Ragged batches.  No counterpart in the reference, whose callers create
  * one context per transform size and loop over the transforms
  * (fft_init_full + fft_execute_batched per size).  A plan covers `count`

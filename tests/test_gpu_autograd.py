@@ -312,3 +312,62 @@ def test_phase_recovery_beside_griffin_lim():
           f"Griffin-Lim x100 {sc_gl:.4f}")
     assert sc_grad < 0.5 * hist[0]
     assert np.isfinite(sc_gl)
+
+
+@pytest.mark.parametrize("S,L,N,W,H,kind", [(2, 9000, 256, 256, 64, "hann"), (3, 5000, 64, 48, 16, "hamming"),
+                                            (4, 20000, 1024, 1024, 256, "hann"), (2, 40000, 2048, 2048, 512, "hann"),
+                                            (1, 70000, 16384, 16384, 4096, "hann"), (2, 3000, 16, 16, 4, None),
+                                            (3, 50, 64, 64, 16, "hann")])
+def test_fused_l2_loss_matches_fp64(S, L, N, W, H, kind):
+    """stft_magnitude_l2_loss: the loss sum((|X| - T)^2) against FP64 and its
+    gradient (one fused forward kernel, the scaled adjoint kernel) against
+    the FP64 gradient 2 (|X| - T) d|X|/dx, with an upstream gradient that
+    stays on the device; the target's gradient -2 (|X| - T)."""
+    x = sinusoids(S, L, 300 + N)
+    y = sinusoids(S, L, 400 + N)
+    win = window_of(kind, W)
+    M64 = grad64.stft_mag64(x, N, W, H, win)
+    T = grad64.stft_mag64(y, N, W, H, win).astype(np.float32)
+    plan = ag.StftPlan(N, H, W, kind)
+    xt = torch.from_numpy(x).cuda().requires_grad_(True)
+    tt = torch.from_numpy(T).cuda().requires_grad_(True)
+    loss = ag.stft_magnitude_l2_loss(xt, tt, plan)
+    up = torch.tensor(0.75, device="cuda")
+    loss.backward(up)
+    ref_loss = float(((M64 - T.astype(np.float64)) ** 2).sum())
+    assert abs(float(loss) - ref_loss) <= tol(N) * ref_loss
+    g64 = 2.0 * 0.75 * (M64 - T.astype(np.float64))
+    ref = grad64.stft_mag_grad64(x, g64, N, W, H, win)
+    assert rel_l2(xt.grad.cpu().numpy(), ref) <= tol(N)
+    assert rel_l2(tt.grad.cpu().numpy(), -g64) <= tol(N)
+    # the same loss through the unfused path (magnitude + torch ops)
+    xt2 = torch.from_numpy(x).cuda().requires_grad_(True)
+    l2 = (ag.stft_magnitude(xt2, plan) - tt.detach()).square().sum()
+    l2.backward(up)
+    assert abs(float(l2) - float(loss)) <= tol(N) * float(loss)
+    assert rel_l2(xt.grad.cpu().numpy(), xt2.grad.cpu().numpy()) <= tol(N)
+    plan.close()
+
+
+def test_fused_l2_loss_deterministic_and_budget_fallback():
+    """Two runs give the same loss and gradient bits; a plan whose phase
+    budget is exceeded takes the unfused path with the same result."""
+    S, L, N, H = 2, 40000, 2048, 512
+    x = torch.from_numpy(sinusoids(S, L, 7)).cuda()
+    plan = ag.StftPlan(N, H, N, "hann")
+    T = plan.magnitude(x.roll(1, 0)).detach()
+    outs = []
+    for _ in range(2):
+        xr = x.clone().requires_grad_(True)
+        loss = ag.stft_magnitude_l2_loss(xr, T, plan)
+        loss.backward()
+        outs.append((float(loss), xr.grad.clone()))
+    assert outs[0][0] == outs[1][0] and torch.equal(outs[0][1], outs[1][1])
+    small = ag.StftPlan(N, H, N, "hann", phase_budget=0)
+    xr = x.clone().requires_grad_(True)
+    loss = ag.stft_magnitude_l2_loss(xr, T, small)
+    loss.backward()
+    assert abs(float(loss) - outs[0][0]) <= tol(N) * outs[0][0]
+    assert rel_l2(xr.grad.cpu().numpy(), outs[0][1].cpu().numpy()) <= tol(N)
+    plan.close()
+    small.close()
