@@ -271,8 +271,11 @@ static bool single_pass(int N, bool real_input) {
 }
 
 static float2* scratch_for(FftContext* c, int N, long long batch, size_t* chunk) {
-  const size_t points = four_step_scratch(ilog2((size_t)N), batch, chunk);
-  return static_cast<float2*>(c->d_scratch.get(points * sizeof(float2)));
+  *chunk = four_step_chunk(ilog2((size_t)N), batch);
+  // two slots when the multi-pass pipeline alternates between chunks,
+  // one when a single chunk covers the batch
+  const size_t slots = ((long long)*chunk < batch) ? 2 : 1;
+  return static_cast<float2*>(c->d_scratch.get(slots * *chunk * (size_t)N * sizeof(float2)));
 }
 
 static void setup_device(FftContext* c) {

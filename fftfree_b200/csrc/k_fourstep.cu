@@ -21,8 +21,6 @@
 
 namespace ffb {
 
-bool tc16_requested();
-
 namespace {
 
 // Shared tile stride per group: padded, and 1 mod 16 so that lanes of
@@ -116,114 +114,14 @@ k_four_b(IO io, const float2* __restrict__ scratch, long long b0, int LN, Twiddl
   }
 }
 
+template <int LN1>
+using SubSched = Sched<LN1, 4>;
+
 template <class S>
 cudaError_t set_smem(const void* fn, size_t bytes) {
   if (bytes > 48 * 1024) return cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
   return cudaSuccess;
 }
-
-// ---------------------------------------------------------------- fused form
-// N = 16 * N2 (N2 = N / 16 <= 4096) in ONE persistent kernel, a transform at
-// a time per block of 1024 threads (one block per SM):
-//   pass A: x[n1 N2 + n2] -> the 16-point DFT over n1 in registers (each
-//     thread a column n2, loads coalesced across the block), times w_N^(n2 k1),
-//     into the block's scratch slot as rows k1 of N2 points;
-//   pass B: the 16 rows through the single-pass engine, G = 1024 / T rows at a
-//     time; X[k1 + 16 k2] leaves straight from registers -- the G rows of one
-//     round fill whole 32-byte sectors of the output.
-// The slot (N points) is rewritten by the block's next transform right away,
-// so the scratch of all blocks (148 x N points, 74 MB at N = 65536) stays in
-// L2: HBM sees the input once and the output once.
-constexpr int kFusedBlock = 1024;
-constexpr int kFusedMaxLog = 16;
-
-template <int LN>
-struct FusedRows {
-  static constexpr int LN2 = LN - 4;
-  // pass radix of the rows: T = N2 / R kept out of (32, 128) (named barriers)
-  static constexpr int LR = (LN2 == 10) ? 3 : 4;
-  using S = Sched<LN2, LR>;
-  static constexpr int G = kFusedBlock / S::T;  // rows per round
-};
-
-template <int LN, class IO>
-__global__ void __launch_bounds__(kFusedBlock, 1) k_four_fused(IO io, float2* __restrict__ scratch, long long batch,
-                                                                Twiddles tw) {
-  extern __shared__ float2 smem[];
-  using FR = FusedRows<LN>;
-  using S2 = typename FR::S;
-  constexpr int N2 = 1 << FR::LN2, T2 = S2::T, G = FR::G;
-  static_assert(16 % G == 0 && G >= 4, "rounds of whole sectors");
-  float2* scr = scratch + (long long)blockIdx.x * (1LL << LN);
-  const int g = threadIdx.x / T2;
-  const int t = threadIdx.x - g * T2;
-  for (long long b = blockIdx.x; b < batch; b += gridDim.x) {
-    // pass A: column n2, 16 points in registers
-#pragma unroll 1
-    for (int n2 = threadIdx.x; n2 < N2; n2 += kFusedBlock) {
-      float2 v[16];
-#pragma unroll
-      for (int n1 = 0; n1 < 16; ++n1) v[n1] = io.elem4(b, (long long)n1 * N2 + n2);
-      Dft<16>::run(v);
-      scr[n2] = v[0];
-#pragma unroll
-      for (int k1 = 1; k1 < 16; ++k1) scr[(long long)k1 * N2 + n2] = cmul(v[k1], tw_split(tw, LN, (unsigned)(n2 * k1)));
-    }
-    __syncthreads();
-    // pass B: rows k1 = r0 + g
-#pragma unroll 1
-    for (int r0 = 0; r0 < 16; r0 += G) {
-      const int k1 = r0 + g;
-      float2 v[S2::R];
-      const float2* row = scr + (long long)k1 * N2;
-#pragma unroll
-      for (int i = 0; i < S2::R; ++i) v[i] = row[t + i * T2];
-      fft_engine<S2, GroupSync>(v, t, smem + g * S2::SMEM, tw);
-#pragma unroll
-      for (int i = 0; i < S2::R; ++i) io.emit4(b, (long long)k1 + 16LL * (t + i * T2), v[i]);
-    }
-    __syncthreads();  // the slot and the tiles are reused by the next transform
-  }
-}
-
-// FFTFREE_FOURSTEP_FUSED=0 selects the two-kernel pipeline for every size.
-bool fused_wanted() {
-  static const bool on = [] {
-    const char* e = std::getenv("FFTFREE_FOURSTEP_FUSED");
-    return !(e && e[0] == '0');
-  }();
-  return on;
-}
-
-int fused_grid() {
-  static int grid[64] = {};
-  int dev = 0;
-  cudaGetDevice(&dev);
-  int& g = grid[dev & 63];
-  if (!g) {
-    int sms = 0;
-    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    g = sms > 0 ? sms : 1;
-  }
-  return g;
-}
-
-template <int LN, class IO>
-cudaError_t run_fused(const IO& io, long long batch, float2* scratch, cudaStream_t st, uint64_t* launches) {
-  using FR = FusedRows<LN>;
-  const size_t sm = (size_t)FR::G * FR::S::SMEM * sizeof(float2);
-  cudaError_t e = set_smem<typename FR::S>((const void*)k_four_fused<LN, IO>, sm);
-  if (e != cudaSuccess) return e;
-  Twiddles tw{twiddle_pyramid(LN, st), twiddle_pass_tables(st)};
-  const long long grid = std::min<long long>(batch, fused_grid());
-  k_four_fused<LN, IO><<<(unsigned)grid, kFusedBlock, sm, st>>>(io, scratch, batch, tw);
-  if (launches) ++*launches;
-  return cudaGetLastError();
-}
-
-template <int LN1>
-using SubSched = Sched<LN1, 4>;
-
 
 // Two-stream software pipeline over chunks: pass A of chunk i+1 (stream
 // sa) overlaps pass B of chunk i (stream sb); the two scratch slots
@@ -314,14 +212,6 @@ cudaError_t run_four(const IO& io, long long batch, float2* scratch, long long c
 template <class IO, bool TC = false>
 cudaError_t four_dispatch(const IO& io, int LN, long long batch, float2* scratch, long long chunk,
                           cudaStream_t st, uint64_t* l) {
-  if (!TC && fused_wanted() && LN <= kFusedMaxLog) {
-    switch (LN) {
-      case 14: return run_fused<14>(io, batch, scratch, st, l);
-      case 15: return run_fused<15>(io, batch, scratch, st, l);
-      case 16: return run_fused<16>(io, batch, scratch, st, l);
-      default: break;
-    }
-  }
   switch (LN) {
     case 14: return run_four<7, 7, IO, TC>(io, batch, scratch, chunk, st, l);
     case 15: return run_four<8, 7, IO, TC>(io, batch, scratch, chunk, st, l);
@@ -338,20 +228,7 @@ cudaError_t four_dispatch(const IO& io, int LN, long long batch, float2* scratch
 
 int max_multi_pass_log() { return 20; }
 
-// Scratch (complex points) a multi-pass call needs: the fused form one slot
-// per persistent block, the two-kernel pipeline two slots of `chunk`
-// transforms (one when a chunk covers the batch).
-size_t four_step_scratch(int LN, long long batch, size_t* chunk) {
-  const long long n = 1LL << LN;
-  if (fused_wanted() && LN <= kFusedMaxLog && !(tc16_requested() && LN >= 15)) {
-    *chunk = (size_t)std::min<long long>(std::max<long long>(batch, 1), fused_grid());
-    return *chunk * (size_t)n;
-  }
-  *chunk = four_step_chunk(LN, batch);
-  const size_t slots = ((long long)*chunk < batch) ? 2 : 1;
-  return slots * *chunk * (size_t)n;
-}
-
+// Scratch is sized for two slots of `chunk` transforms (see run_four).
 size_t four_step_chunk(int LN, long long batch) {
   // Scratch budget per chunk (MB; FFTFREE_FOURSTEP_CHUNK_MB overrides it).
   // B200 sweeps: one large chunk beats L2-sized chunks, whose one-wave

@@ -226,9 +226,6 @@ cudaError_t launch_ragged(const RaggedArgs& a, int grid, cudaStream_t s, uint64_
 // that stays resident in L2).
 int max_multi_pass_log();
 size_t four_step_chunk(int log_n, long long batch);
-// Complex points of scratch a multi-pass call over `batch` transforms of
-// 2^log_n points needs, and the `chunk` to pass to the launchers.
-size_t four_step_scratch(int log_n, long long batch, size_t* chunk);
 cudaError_t launch_four_step_stft(const StftArgs& a, float2* scratch, size_t chunk, cudaStream_t s,
                                   uint64_t* launches);
 cudaError_t launch_four_step_c2c(const C2cArgs& a, float2* scratch, size_t chunk, cudaStream_t s,
