@@ -194,6 +194,7 @@ CASES = {
     "mag_n2048": "magnitude STFT N=W=2048 H=512, 64 x 262144 samples (autograd plain forward)",
     "mag_phasor_n2048": "magnitude + unit phasor STFT N=W=2048 H=512, 64 x 262144 samples (autograd forward)",
     "grad_phasor_n2048": "magnitude STFT gradient from the saved phasor, N=W=2048 H=512, 64 x 262144",
+    "mag_l2_n2048": "fused spectral L2 loss forward (residual, phasor, partial sums), N=W=2048 H=512, 64 x 262144",
     "grad_recompute_n2048": "magnitude STFT gradient with the spectrum recomputed, N=W=2048 H=512, 64 x 262144",
     "c2c_n65536_b512": "C2C N=65536 x 512 complex64, four-step (two passes)",
     "ragged_4096": "ragged batch: 4096 R2C signals, N = 2^e, e uniform in 6..16 (seed 2), one persistent launch",
@@ -280,7 +281,9 @@ def run_case(args):
         up = torch.randn(S, F, bins, device="cuda", generator=g)
         ph = plan.magnitude_phasor(x)[1]
         spec = S * F * bins * 4
+        tgt = torch.rand(S, F, bins, device="cuda", generator=g)
         fn, nbytes = {
+            "mag_l2_n2048": (lambda: plan.magnitude_l2(x, tgt), S * L * 4 + 4 * spec),
             "mag_n2048": (lambda: plan.magnitude(x), S * L * 4 + spec),
             "mag_phasor_n2048": (lambda: plan.magnitude_phasor(x), S * L * 4 + 3 * spec),
             "grad_phasor_n2048": (lambda: plan.magnitude_backward_phasor(ph, up, L), 3 * spec + S * L * 4),
