@@ -319,6 +319,17 @@ struct StftIO {
   __device__ __forceinline__ void store(long long f, int t, float2 (&v)[S::R], float2* sm,
                                         const Twiddles& tw) const {
     constexpr int M = S::M, T = S::T, R = S::R;
+    // L2 loss: the frame's target row is fetched first, so that its loads
+    // are in flight across the tile exchange
+    float tgv[MODE == 5 ? R : 1];
+    float tg_nyq = 0.f;
+    if constexpr (MODE == 5) {
+      const bool okf = f < a.frames;
+      const float* tg = a.target + (okf ? f : 0) * a.out_stride + t;
+#pragma unroll
+      for (int i = 0; i < R; ++i) tgv[i] = okf ? __ldg(tg + i * T) : 0.f;
+      if (t == 0 && okf) tg_nyq = __ldg(a.target + f * a.out_stride + M);
+    }
     tile_write_natural<S>(v, t, sm);
     GroupSync::sync<S>();
     if (f >= a.frames) return;
@@ -342,7 +353,6 @@ struct StftIO {
       float* pi = im + t;
       float* pm = mg + t;
       if constexpr (MODE == 5) {
-        const float* tg = a.target + ob + t;
         float2* ph = reinterpret_cast<float2*>(re) + t;
         float acc = 0.f;
 #pragma unroll
@@ -352,14 +362,14 @@ struct StftIO {
           if (i == 0 && t == 0) X.y = 0.f;  // DC
           float m;
           ph[i * T] = mag_phasor(X, &m);
-          const float r = m - __ldg(tg + i * T);
+          const float r = m - tgv[i];
           pm[i * T] = r;
           acc = __fmaf_rn(r, r, acc);
         }
         if (t == 0) {  // Nyquist X[M] = Re Z[0] - Im Z[0]
           float m;
           reinterpret_cast<float2*>(re)[M] = mag_phasor(make_float2(v[0].x - v[0].y, 0.f), &m);
-          const float r = m - __ldg(a.target + ob + M);
+          const float r = m - tg_nyq;
           mg[M] = r;
           acc = __fmaf_rn(r, r, acc);
         }
