@@ -595,8 +595,7 @@ struct C2rHalfIO {
   // X[k] as the Hermitian rebuild sees it (fft_cffi.cpp:1073-1078, and the
   // Cooley-Tukey pre-hook's polar conversion eigen_fft.hpp:2511-2522),
   // conjugated for a forward context.
-  __device__ __forceinline__ float2 bin(const float* re, const float* im, int k, bool edge, float cs) const {
-    float2 u = make_float2(__ldg(re + k), __ldg(im + k));
+  __device__ __forceinline__ float2 bin_of(float2 u, bool edge, float cs) const {
     if (edge) u.y = 0.f;
     if (a.ct_pre == 2 && a.polar_in) {
       u = polar_to_complex(u);
@@ -617,13 +616,19 @@ struct C2rHalfIO {
       const float* re = a.in_re + f * (long long)a.bins;
       const float* im = a.in_im + f * (long long)a.bins;
       const float cs = a.inverse ? 1.f : -1.f;  // forward: conjugate spectrum
+      // every load of the frame first (in flight together), then the
+      // conversions and the tile writes
+#pragma unroll
+      for (int i = 0; i < R; ++i) xk[i] = make_float2(__ldg(re + t + i * T), __ldg(im + t + i * T));
+      float2 xn = make_float2(0.f, 0.f);
+      if (t == 0) xn = make_float2(__ldg(re + M), __ldg(im + M));
 #pragma unroll
       for (int i = 0; i < R; ++i) {
         const int k = t + i * T;
-        xk[i] = bin(re, im, k, k == 0, cs);
+        xk[i] = bin_of(xk[i], k == 0, cs);
         sm[pidx(k)] = xk[i];
       }
-      if (t == 0) sm[pidx(M)] = bin(re, im, M, true, cs);
+      if (t == 0) sm[pidx(M)] = bin_of(xn, true, cs);
     }
     GroupSync::sync<S>();
     const UntangleTw<S> w(tw, t);

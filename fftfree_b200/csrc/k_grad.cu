@@ -154,18 +154,18 @@ __device__ __forceinline__ void grad_inverse(const MagGradArgs& a, const float2 
   GroupSync::sync<S>();  // the engine reuses the tile
   fft_engine<S, GroupSync>(v, t, sm, tw);
 
-  // dL/ds[2m] = Re, dL/ds[2m+1] = -Im, times the window, zero past the frame's samples.
+  // dL/ds[2m] = Re, dL/ds[2m+1] = -Im, times the window (taps 2m, 2m + 1 as
+  // one 8-byte load: the context's device window is N floats, 256-byte
+  // aligned), zero past the frame's samples.
+  const float2* w2 = reinterpret_cast<const float2*>(a.win);
 #pragma unroll
   for (int i = 0; i < R; ++i) {
     const int n = 2 * (t + i * T);
-    float d0 = v[i].x, d1 = -v[i].y;
-    if (a.win) {
-      d0 *= __ldg(a.win + n);
-      d1 *= __ldg(a.win + n + 1);
-    }
-    if (n >= cnt) d0 = 0.f;
-    if (n + 1 >= cnt) d1 = 0.f;
-    v[i] = make_float2(d0, d1);
+    float2 d = make_float2(v[i].x, -v[i].y);
+    if (w2) d = __fmul2_rn(d, __ldg(w2 + (t + i * T)));
+    if (n >= cnt) d.x = 0.f;
+    if (n + 1 >= cnt) d.y = 0.f;
+    v[i] = d;
   }
 }
 
