@@ -281,7 +281,7 @@ def test_recovery_coordinator_matches_reference(name, setup, frames):
     pcm = np.random.default_rng(frames).uniform(-1, 1, N * frames).astype(np.float32)
     R = reflib.lib()
     _, ore, _, _ = oracle_for(kw).execute_batched(pcm)
-    for _ in range(3):
+    for _ in range(8):
         _reset(R)
         setup(R)
         reflib.observer_attach(R)
