@@ -260,7 +260,7 @@ def test_recovery_coordinator_matches_reference(name, setup, frames):
     2-thread WorkerPool: the same restore-observer calls and the same frames
     given up (left as their restored input in the reference's output).  The
     reference's pool is not deterministic under every mode, so it gets up to
-    three runs to produce the coordinator's calls."""
+    eight runs to produce the coordinator's outcome."""
     import ctypes
     import fftfree_b200 as ff
     ours = []
