@@ -110,7 +110,7 @@ __device__ __forceinline__ void ragged_split(const RaggedArgs& a, int4 tile, flo
   constexpr int T = S::T, R = S::R, MQ = S::M, M = P * MQ, LM = kSubLog + (P == 2 ? 1 : 2);
   static_assert(T == kBlock, "the whole block per sub-transform");
   const int t = threadIdx.x;
-  float2* scr = a.scratch + (long long)blockIdx.x * M;
+  float2* scr = a.scratch + (long long)blockIdx.x * (1LL << kMaxLog);  // the block's slot (the largest size)
   // sub-transform q: the first reads the frame once -- z[P n] into the
   // registers, z[P n + q'] (q' > 0) into slot q' -- the others their slot
   // (each thread reads only its own points before the engine's first
