@@ -7,28 +7,28 @@
 // mag) rows of N_i/2 + 1 bins are concatenated in item order.  Every frame
 // is one job; the host groups the jobs of one size into tiles, largest
 // first (longest processing time first balances the persistent blocks), and
-// the blocks (512 threads, two per SM, so that one block's loads overlap the
-// other's transforms) take tiles from an atomic counter until the list is
-// exhausted.  A tile is
-//  * a group of same-size frames of up to 2^13 complex points, one per
+// the blocks (1024 threads, one per SM) take tiles from an atomic counter
+// until the list is exhausted.  A tile is
+//  * a group of same-size frames of up to 2^14 complex points, one per
 //    T-thread slice of the block -- the single-pass engine and the STFT
 //    load / store policy of fft_execute_batched, so a frame matches that
-//    call bit for bit where the radix is the same;
-//  * one frame of 2^14 or 2^15 complex points (N = 32768, 65536), beyond one
-//    block's shared memory: a decimation-in-time split into P = 2 or 4
-//    transforms of 2^13 points run one after the other through the block's
-//    engine, the frame read once, the pending points and spectra in a
-//    scratch slot of the block (2^15 points, 256 KB; 296 slots, 76 MB:
-//    L2-resident), and a combine step that untangles bins k + (M/P) j for all
-//    j together so that the outputs stay contiguous.
+//    call bit for bit where the radix is the same; 2^14 points take the
+//    whole block (T = 1024, the transform held in registers and 139 KB of
+//    shared memory);
+//  * one frame of 2^15 complex points (N = 65536), which exceeds one SM's
+//    shared memory: a decimation-in-time split into two 2^14-point
+//    transforms of the even and odd points, run one after the other through
+//    the block's engine; the first half's spectrum waits in a 128 KB scratch
+//    slot of the block (148 slots, 19 MB: L2-resident), and the combine step
+//    untangles bins k and k + M/2 together so the outputs stay contiguous.
 #include "fft_launch.cuh"
 
 namespace ffb {
 namespace {
 
-constexpr int kBlock = 512;
-constexpr int kSubLog = 13;    // log2 complex points of one block's single pass
-constexpr int kMaxLog = 15;    // log2 complex points of the largest item
+constexpr int kBlock = 1024;
+constexpr int kSplitLog = 15;  // log2 complex points of the two-half path
+constexpr int kFullLog = 14;   // one-block single pass
 
 // ---------------------------------------------------------------- single-pass tile
 template <class S, int MODE>
@@ -63,7 +63,7 @@ __device__ __forceinline__ void ragged_single(const RaggedArgs& a, int4 tile, fl
   io.template store<S>(job.y, t, v, sm, tw);
 }
 
-// ---------------------------------------------------------------- split tile
+// ---------------------------------------------------------------- two-half tile
 // Samples j, j + 1 of the windowed, zero-padded frame.
 __device__ __forceinline__ float2 frame_pair(const float* src, const float* win, long long cnt, long long j,
                                              bool fast) {
@@ -78,80 +78,56 @@ __device__ __forceinline__ float2 frame_pair(const float* src, const float* win,
   return make_float2(x0, x1);
 }
 
-// exp(-2 pi i q / P) for q < P (P = 2 or 4): 1, -1 / 1, -i, -1, i.
-template <int P>
-__device__ __forceinline__ float2 root_p(int q) {
-  if constexpr (P == 2) return make_float2(q ? -1.f : 1.f, 0.f);
-  return wconst<4>(q);
-}
-
-// M = P * 2^13 complex points z[m] = (s[2m], s[2m+1]) of an N = 2M frame, by
-// decimation in time: E_q = DFT_{M/P}(z[P n + q]), then for k < M/P
-//   Z[k + (M/P) j] = sum_q exp(-2 pi i q j / P) w_M^(q k) E_q[k],
-// and X[k + (M/P) j] = untangle(Z[k + (M/P) j], Z[M - k - (M/P) j]).  The frame is
-// read once (the P points z[P n .. P n + P - 1] of each n together): z[P n]
-// stays in registers for the first transform, the others wait in the block's
-// scratch slot (M points) and are transformed there in place; the last
-// spectrum goes to the tile.  The combine reads E_q at k and M/P - k and
-// writes bins k + (M/P) j for every j: contiguous across the block's lanes.
-template <int P, class S>
-__device__ __forceinline__ void split_frame(const RaggedArgs& a, int4 tile, const float** src, const float** win,
-                                            long long* cnt, bool* fast) {
+// M = 2^15 complex points z[m] = (s[2m], s[2m+1]) of an N = 2^16 frame:
+// E = DFT_{M/2}(z[2n]), O = DFT_{M/2}(z[2n+1]),
+// Z[k] = E[k] + w_M^k O[k], Z[k + M/2] = E[k] - w_M^k O[k]; then
+// X[k] = untangle(Z[k], Z[M - k]) and X[k + M/2] = untangle(Z[k + M/2], Z[M/2 - k]).
+// The points z[2n + odd] of the tile's frame into v (n = t + i T).  The
+// frame's bookkeeping is re-read for each half, so that nothing but the tile
+// stays live across the engine (a 2^14-point engine at 1024 threads uses the
+// whole register budget).
+template <class S>
+__device__ __forceinline__ void split_load(const RaggedArgs& a, int4 tile, int odd, int t, float2 (&v)[S::R]) {
+  constexpr int T = S::T, R = S::R, N = 4 * S::M;
   const int2 job = __ldg(a.jobs + tile.x);
   const RaggedItem it = a.items[job.x];
-  *src = stft_frame(a.pcm + it.pcm_off, it.pcm_len, 0, 0, it.W, it.H, job.y, cnt);
-  *win = it.win_off >= 0 ? a.windows + it.win_off : nullptr;
-  *fast = *cnt == 2LL * P * S::M && aligned8(*src) && (!*win || aligned8(*win));
+  long long cnt;
+  const float* src = stft_frame(a.pcm + it.pcm_off, it.pcm_len, 0, 0, it.W, it.H, job.y, &cnt);
+  const float* win = it.win_off >= 0 ? a.windows + it.win_off : nullptr;
+  const bool fast = cnt == (long long)N && aligned8(src) && (!win || aligned8(win));
+#pragma unroll
+  for (int i = 0; i < R; ++i) v[i] = frame_pair(src, win, cnt, 4LL * (t + i * T) + 2 * odd, fast);
 }
 
-template <int P, int MODE>
+template <int MODE>
 __device__ __forceinline__ void ragged_split(const RaggedArgs& a, int4 tile, float2* smem, const Twiddles& tw) {
-  using S = Sched<kSubLog, 4>;
-  constexpr int T = S::T, R = S::R, MQ = S::M, M = P * MQ, LM = kSubLog + (P == 2 ? 1 : 2);
-  static_assert(T == kBlock, "the whole block per sub-transform");
+  using S = Sched<kSplitLog - 1, 4>;
+  constexpr int T = S::T, R = S::R, MH = S::M, M = 2 * MH, LM = kSplitLog;
+  static_assert(T == kBlock, "the whole block per half");
   const int t = threadIdx.x;
-  float2* scr = a.scratch + (long long)blockIdx.x * (1LL << kMaxLog);  // the block's slot (the largest size)
-  // sub-transform q: the first reads the frame once -- z[P n] into the
-  // registers, z[P n + q'] (q' > 0) into slot q' -- the others their slot
-  // (each thread reads only its own points before the engine's first
-  // barrier); spectra back into the slots, the last one into the tile.  One
-  // engine body for all of them (a second copy would keep the first one's
-  // address arithmetic live, beyond the register budget).
+
+  // even points: E, into the block's scratch slot; then the odd points: O,
+  // into the tile (the engine's barriers also order the scratch writes
+  // before the combine's reads).  One engine body for both halves.
 #pragma unroll 1
-  for (int q = 0; q < P; ++q) {
+  for (int odd = 0; odd < 2; ++odd) {
     float2 v[R];
-    if (q == 0) {
-      const float* src;
-      const float* win;
-      long long cnt;
-      bool fast;
-      split_frame<P, S>(a, tile, &src, &win, &cnt, &fast);
-#pragma unroll
-      for (int i = 0; i < R; ++i) {
-        const int n = t + i * T;
-#pragma unroll
-        for (int qq = 0; qq < P; ++qq) {
-          const float2 z = frame_pair(src, win, cnt, 2LL * (P * (long long)n + qq), fast);
-          if (qq == 0) v[i] = z;
-          else scr[qq * MQ + n] = z;
-        }
-      }
-    } else {
-#pragma unroll
-      for (int i = 0; i < R; ++i) v[i] = scr[q * MQ + t + i * T];
-    }
+    split_load<S>(a, tile, odd, t, v);
     fft_engine<S, GroupSync>(v, t, smem, tw);
-    if (q == P - 1) {
+    if (odd) {
       tile_write_natural<S>(v, t, smem);
     } else {
+      float2* scr = a.scratch + (long long)blockIdx.x * MH;
 #pragma unroll
-      for (int i = 0; i < R; ++i) scr[q * MQ + t + i * T] = v[i];
+      for (int i = 0; i < R; ++i) scr[t + i * T] = v[i];
     }
   }
   __syncthreads();
 
   const int2 job = __ldg(a.jobs + tile.x);
   const RaggedItem it = a.items[job.x];
+  const float2* scr = a.scratch + (long long)blockIdx.x * MH;
+
   StftArgs sa{};
   sa.N = 2 * M;
   sa.pf = a.pf;
@@ -161,54 +137,40 @@ __device__ __forceinline__ void ragged_split(const RaggedArgs& a, int4 tile, flo
   float* re = a.out_re + it.out_off + (long long)job.y * (M + 1);
   float* im = a.out_im + it.out_off + (long long)job.y * (M + 1);
   float* mg = a.out_mag + it.out_off + (long long)job.y * (M + 1);
-  // E_q of bin k: the last one from the tile, the others from their slots
-  const auto E = [&](int q, int k) -> float2 { return q == P - 1 ? smem[pidx(k)] : scr[q * MQ + k]; };
-#pragma unroll 1
+#pragma unroll 2
   for (int i = 0; i < R; ++i) {
     const int k = t + i * T;
-    float2 A[P], B[P];
-    float2 wq[P];  // w_M^(q k)
-#pragma unroll
-    for (int q = 0; q < P; ++q) {
-      wq[q] = q ? tw_get(tw, LM, (unsigned)(q * k)) : make_float2(1.f, 0.f);
-      A[q] = q ? cmul(E(q, k), wq[q]) : E(0, k);
-    }
-    if constexpr (P == 2) {
-      Dft<2>::run(A);
+    const float2 wk = tw_get(tw, LM, (unsigned)k);      // w_M^k
+    const float2 e = scr[k];
+    const float2 o = cmul(smem[pidx(k)], wk);  // O[k] (from the tile: the registers go to the combine)
+    const float2 zk = cadd(e, o);                       // Z[k]
+    const float2 zk2 = csub(e, o);                      // Z[k + M/2]
+    float2 zmk, zmk2;                                   // Z[M - k], Z[M/2 - k]
+    if (k == 0) {
+      zmk = zk;
+      zmk2 = zk2;
     } else {
-      Dft<4>::run(A);
-    }
-    if (k > 0) {
-      // w_M^(q (M/P - k)) = exp(-2 pi i q / P) conj(w_M^(q k))
-#pragma unroll
-      for (int q = 0; q < P; ++q)
-        B[q] = q ? cmul(E(q, MQ - k), cmul(root_p<P>(q), cconj(wq[q]))) : E(0, MQ - k);
-      if constexpr (P == 2) {
-        Dft<2>::run(B);
-      } else {
-        Dft<4>::run(B);
-      }
+      const float2 wm = make_float2(-wk.x, wk.y);       // w_M^(M/2 - k) = -conj(w_M^k)
+      const float2 om = cmul(smem[pidx(MH - k)], wm);
+      const float2 em = scr[MH - k];
+      zmk2 = cadd(em, om);
+      zmk = csub(em, om);
     }
     const float2 wn = tw_get(tw, LM + 1, (unsigned)k);  // w_N^k
-#pragma unroll
-    for (int j = 0; j < P; ++j) {
-      // partner Z[M - k - (M/P) j]: B[P-1-j] (k > 0), A[(P - j) mod P] (k = 0)
-      const float2 zm = k ? B[P - 1 - j] : A[(P - j) & (P - 1)];
-      const float2 c = wconst<2 * P>(j);  // w_N^((M/P) j)
-      const float2 h = make_float2(0.5f * (wn.x * c.x - wn.y * c.y), 0.5f * (wn.x * c.y + wn.y * c.x));
-      float2 X = untangle_bin(A[j], zm, h);
-      if (k == 0 && j == 0) X.y = 0.f;  // DC
-      io.emit(re, im, mg, k + MQ * j, X, k == 0 && j == 0, 1.0f, mag_is_re);
-    }
-    if (k == 0) io.emit(re, im, mg, M, make_float2(A[0].x - A[0].y, 0.f), true, 1.0f, mag_is_re);  // Nyquist
+    const float2 h = make_float2(0.5f * wn.x, 0.5f * wn.y);
+    const float2 h2 = make_float2(0.5f * wn.y, -0.5f * wn.x);  // w_N^(k + M/2) / 2 = -i w_N^k / 2
+    float2 X = untangle_bin(zk, zmk, h);
+    if (k == 0) X.y = 0.f;  // DC
+    io.emit(re, im, mg, k, X, k == 0, 1.0f, mag_is_re);
+    io.emit(re, im, mg, k + MH, untangle_bin(zk2, zmk2, h2), false, 1.0f, mag_is_re);
+    if (k == 0) io.emit(re, im, mg, M, make_float2(zk.x - zk.y, 0.f), true, 1.0f, mag_is_re);  // Nyquist
   }
   __syncthreads();  // shared memory and scratch are reused by the block's next tile
 }
 
 // ---------------------------------------------------------------- dispatch
-// tile.z = log2 complex points, tile.w = pass radix (log2), 0 for the split
-// paths; the pass radices keep T = M / R <= 32 or >= 64 (named barriers per
-// group: 8 at most in a 512-thread block).
+// tile.z = log2 complex points, tile.w = pass radix (log2); the pass radices
+// keep T = M / R out of (32, 128) (named barriers per group: 15 at most).
 template <int MODE>
 __device__ __forceinline__ void ragged_tile(const RaggedArgs& a, int4 tile, float2* smem, const Twiddles& tw) {
 #define FFB_RS(L, R)                                              \
@@ -218,17 +180,16 @@ __device__ __forceinline__ void ragged_tile(const RaggedArgs& a, int4 tile, floa
   switch (tile.z * 8 + tile.w) {
     FFB_RS(1, 2) FFB_RS(2, 2) FFB_RS(3, 2) FFB_RS(4, 2)
     FFB_RS(5, 2) FFB_RS(5, 3) FFB_RS(6, 3) FFB_RS(6, 4) FFB_RS(7, 3) FFB_RS(7, 4)
-    FFB_RS(8, 3) FFB_RS(8, 4) FFB_RS(9, 3) FFB_RS(9, 4) FFB_RS(10, 3) FFB_RS(10, 4)
-    FFB_RS(11, 3) FFB_RS(11, 4) FFB_RS(12, 3) FFB_RS(12, 4) FFB_RS(13, 4)
-    case (kSubLog + 1) * 8: ragged_split<2, MODE>(a, tile, smem, tw); return;
-    case (kSubLog + 2) * 8: ragged_split<4, MODE>(a, tile, smem, tw); return;
+    FFB_RS(8, 3) FFB_RS(8, 4) FFB_RS(9, 4) FFB_RS(10, 3)
+    FFB_RS(11, 3) FFB_RS(11, 4) FFB_RS(12, 4) FFB_RS(13, 4) FFB_RS(14, 4)
+    case kSplitLog * 8: ragged_split<MODE>(a, tile, smem, tw); return;
     default: return;
   }
 #undef FFB_RS
 }
 
 template <int MODE>
-__global__ void __launch_bounds__(kBlock, 2) k_ragged(RaggedArgs a, Twiddles tw) {
+__global__ void __launch_bounds__(kBlock, 1) k_ragged(RaggedArgs a, Twiddles tw) {
   extern __shared__ float2 smem[];
   __shared__ int next;
   for (;;) {
@@ -251,22 +212,21 @@ constexpr size_t cmax(size_t a, size_t b) { return a > b ? a : b; }
 
 constexpr size_t ragged_smem_bytes() {
   // the largest over the tiles of ragged_tile (small transforms carry more
-  // padding per point: 128 groups of 64 points take the most)
+  // padding per point: 256 groups of 64 points take the most)
   return cmax(cmax(cmax(cmax(tile_smem<1, 2>(), tile_smem<2, 2>()), cmax(tile_smem<3, 2>(), tile_smem<4, 2>())),
                    cmax(cmax(tile_smem<5, 2>(), tile_smem<5, 3>()), cmax(tile_smem<6, 3>(), tile_smem<6, 4>()))),
               cmax(cmax(cmax(tile_smem<7, 3>(), tile_smem<7, 4>()), cmax(tile_smem<8, 3>(), tile_smem<8, 4>())),
-                   cmax(cmax(cmax(tile_smem<9, 3>(), tile_smem<9, 4>()), cmax(tile_smem<10, 3>(), tile_smem<10, 4>())),
-                        cmax(cmax(tile_smem<11, 3>(), tile_smem<11, 4>()),
-                             cmax(cmax(tile_smem<12, 3>(), tile_smem<12, 4>()), tile_smem<13, 4>())))));
+                   cmax(cmax(cmax(tile_smem<9, 4>(), tile_smem<10, 3>()), cmax(tile_smem<11, 3>(), tile_smem<11, 4>())),
+                        cmax(cmax(tile_smem<12, 4>(), tile_smem<13, 4>()), tile_smem<14, 4>()))));
 }
-static_assert(2 * ragged_smem_bytes() <= 226 * 1024, "two blocks per SM");
+static_assert(ragged_smem_bytes() <= 227 * 1024, "one block per SM");
 
 template <int MODE>
 cudaError_t launch_mode(const RaggedArgs& a, int grid, cudaStream_t st, uint64_t* launches) {
   const size_t smem = ragged_smem_bytes();
   cudaError_t e = cudaFuncSetAttribute(k_ragged<MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
-  Twiddles tw{twiddle_pyramid(kMaxLog + 1, st), twiddle_pass_tables(st)};
+  Twiddles tw{twiddle_pyramid(kSplitLog + 1, st), twiddle_pass_tables(st)};
   k_ragged<MODE><<<grid, kBlock, smem, st>>>(a, tw);
   if (launches) ++*launches;
   return cudaGetLastError();
@@ -274,16 +234,18 @@ cudaError_t launch_mode(const RaggedArgs& a, int grid, cudaStream_t st, uint64_t
 
 }  // namespace
 
-int ragged_max_log() { return kMaxLog + 1; }  // log2 N of the largest item
-int ragged_block_log(int logm) { return logm > kSubLog ? 1 : 0; }
-size_t ragged_scratch_per_block() { return (size_t)(1u << kMaxLog) * sizeof(float2); }
+int ragged_max_log() { return kSplitLog + 1; }  // log2 N of the largest item
+int ragged_block_log(int logm) { return logm >= kFullLog ? 1 : 0; }
+size_t ragged_scratch_per_block() { return (size_t)(1u << (kSplitLog - 1)) * sizeof(float2); }
 int ragged_block_threads() { return kBlock; }
 
 int ragged_candidates(int logm, int* lrs) {
-  if (logm > kSubLog) return 0;
+  if (logm >= kSplitLog) return 0;
   if (logm <= 4) { lrs[0] = 2; return 1; }
   if (logm == 5) { lrs[0] = 2; lrs[1] = 3; return 2; }
-  if (logm == kSubLog) { lrs[0] = 4; return 1; }  // T = 512, the whole block
+  if (logm == 9) { lrs[0] = 4; return 1; }   // T = 32 (radix 8 would give T = 64)
+  if (logm == 10) { lrs[0] = 3; return 1; }  // T = 128 (radix 16 would give T = 64)
+  if (logm >= 12) { lrs[0] = 4; return 1; }
   lrs[0] = 3;
   lrs[1] = 4;
   return 2;

@@ -105,7 +105,7 @@ WorkList build_work(const RaggedPlan& p, int only) {
     const int per = whole ? 1 : std::max(1, ragged_block_threads() / T);
     for (size_t s = 0; s < by[L].size(); s += per) {
       const int n = (int)std::min<size_t>(per, by[L].size() - s);
-      const int lr = whole ? 0 : p.lr[L];
+      const int lr = (L == ragged_max_log() - 1) ? 0 : p.lr[L];
       w.tiles.push_back(make_int4((int)w.jobs.size(), n, L, lr));
       for (int k = 0; k < n; ++k) w.jobs.push_back(by[L][s + k]);
     }
@@ -361,7 +361,7 @@ FFT_CFFI_API void* fftfree_ragged_plan_stft(const size_t* n, const size_t* lengt
       RG_CHECK(cudaMemcpyAsync(p->d_windows.get(p->windows.size() * 4), p->windows.data(), p->windows.size() * 4,
                                cudaMemcpyHostToDevice, p->stream));
     bool any_split = false;
-    for (size_t i = 0; i < count; ++i) any_split = any_split || (ragged_block_log(p->logm[i]) && p->frames[i]);
+    for (size_t i = 0; i < count; ++i) any_split = any_split || (p->logm[i] == ragged_max_log() - 1 && p->frames[i]);
     if (any_split) p->d_scratch.get((size_t)p->grid * ragged_scratch_per_block());
     // staging (host buffers) and the tuner's buffers
     RG_CHECK(cudaMemsetAsync(p->d_in.get(std::max<size_t>(1, p->samples) * 4), 0,
@@ -404,7 +404,7 @@ FFT_CFFI_API int fftfree_ragged_schedule(void* plan, size_t n) {
   RaggedPlan* p = as_plan(plan);
   const int lg = log2_exact(n);
   if (!p || lg < 2 || lg > ragged_max_log()) return 0;
-  return ragged_block_log(lg - 1) ? 0 : (1 << p->lr[lg - 1]);
+  return (lg - 1 == ragged_max_log() - 1) ? 0 : (1 << p->lr[lg - 1]);
 }
 
 FFT_CFFI_API void fftfree_ragged_set_stream(void* plan, void* stream) {
