@@ -327,16 +327,16 @@ __global__ void __launch_bounds__(Launch<S>::BLOCK, grad_min_blocks<S>()) k_stft
 // sums are taken in frame order, as in the general form.
 // The sliding form also keeps the register window: 3 blocks of 256 threads
 // (85 registers) at radix 8, 2 (128 registers) at radix 16.
-template <class S, int MB>
+template <class S>
 constexpr int slide_min_blocks() {
-  constexpr int want = MB > 0 ? MB : (S::R <= 8 ? 3 : 2);
+  constexpr int want = S::R <= 8 ? 3 : 2;
   constexpr int fit80 = 65536 / (Launch<S>::BLOCK * 80);  // blocks at 80 registers a thread
   return want < fit80 ? want : (fit80 > 1 ? fit80 : 1);
 }
 
-template <class S, int QL, bool PH, int MB = 0>
-__global__ void __launch_bounds__(Launch<S>::BLOCK, slide_min_blocks<S, MB>()) k_stft_mag_grad_slide(MagGradArgs a,
-                                                                                                     Twiddles tw) {
+template <class S, int QL, bool PH>
+__global__ void __launch_bounds__(Launch<S>::BLOCK, slide_min_blocks<S>()) k_stft_mag_grad_slide(MagGradArgs a,
+                                                                                                 Twiddles tw) {
   extern __shared__ float2 smem[];
   constexpr int T = S::T, R = S::R, M = S::M, G = Launch<S>::G;
   constexpr int SH = R >> QL;  // register slots per hop
@@ -406,22 +406,12 @@ static int slide_logr(int logm) {
   return (logm == 10) ? 4 : 3;
 }
 
-// Blocks per SM the sliding form's registers are sized for at radix 16:
-// FFTFREE_GRAD_BLOCKS=3 caps them at 80 (sweeps).
-static int slide_blocks() {
-  static const int env = [] {
-    const char* e = std::getenv("FFTFREE_GRAD_BLOCKS");
-    return e ? std::atoi(e) : 0;
-  }();
-  return env;
-}
-
-template <class S, int QL, bool PH, int MB>
-static cudaError_t launch_slide_mb(const MagGradArgs& a, cudaStream_t st, uint64_t* launches) {
+template <class S, int QL, bool PH>
+static cudaError_t launch_slide(const MagGradArgs& a, cudaStream_t st, uint64_t* launches) {
   using L = Launch<S>;
   const size_t smem = (size_t)L::G * S::SMEM * sizeof(float2);
   if (smem > 48 * 1024) {
-    const cudaError_t e = cudaFuncSetAttribute(k_stft_mag_grad_slide<S, QL, PH, MB>,
+    const cudaError_t e = cudaFuncSetAttribute(k_stft_mag_grad_slide<S, QL, PH>,
                                                cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
   }
@@ -429,17 +419,9 @@ static cudaError_t launch_slide_mb(const MagGradArgs& a, cudaStream_t st, uint64
   const long long grid = (jobs + L::G - 1) / L::G;
   if (grid > 0x7fffffffLL) return cudaErrorInvalidValue;
   Twiddles tw{twiddle_pyramid(0, st), twiddle_pass_tables(st)};
-  k_stft_mag_grad_slide<S, QL, PH, MB><<<(unsigned)grid, L::BLOCK, smem, st>>>(a, tw);
+  k_stft_mag_grad_slide<S, QL, PH><<<(unsigned)grid, L::BLOCK, smem, st>>>(a, tw);
   if (launches) ++*launches;
   return cudaGetLastError();
-}
-
-template <class S, int QL, bool PH>
-static cudaError_t launch_slide(const MagGradArgs& a, cudaStream_t st, uint64_t* launches) {
-  if constexpr (S::R == 16 && S::LOGM == 10 && QL == 2) {
-    if (slide_blocks() == 3) return launch_slide_mb<S, QL, PH, 3>(a, st, launches);
-  }
-  return launch_slide_mb<S, QL, PH, 0>(a, st, launches);
 }
 
 cudaError_t launch_stft_mag_grad(const MagGradArgs& a, int req_logr, cudaStream_t st, uint64_t* launches) {
