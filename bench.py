@@ -202,6 +202,8 @@ CASES = {
     "r2c_n4096_polar_b8192": "R2C N=W=H=4096, half spectrum, store_polar, 8192 frames (fft_execute_batched)",
     "c2r_n4096_polar_b8192": "C2R N=4096 half spectrum polar input (Cooley-Tukey pre-hook), 8192 frames "
                              "(fft_execute_complex_batched)",
+    "griffin_lim_n1024_h256": "fft_griffin_lim, N=W=1024 H=256 Hann, 4096 frames x 513 bins, 32 iterations "
+                              "(device magnitudes and outputs)",
 }
 
 
@@ -262,6 +264,27 @@ def run_case(args):
             ci.set_async(True)
             out = torch.empty(B * N, device="cuda")
             fn, nbytes = (lambda: ci.execute_complex_batched(re, im, B, out)), 2 * B * bins * 4 + B * N * 4
+    elif name == "griffin_lim_n1024_h256":
+        N, H, F, iters = 1024, 256, 4096, 32
+        bins = N // 2 + 1
+        mag = torch.rand(F * bins, device="cuda", generator=g)
+        re, im = torch.empty_like(mag), torch.empty_like(mag)
+        fc = ff.FftContext.full_v2(N, kernel=2, window=N, hop=H, transform=1, half_spectrum=1, apply_windows=1,
+                                   analysis_kind=1)
+        ic = ff.FftContext.full_v2(N, kernel=2, inverse=1, transform=2, half_spectrum=1, window=N, hop=H)
+        for c in (fc, ic):
+            c.set_stream(stream.cuda_stream)
+        L = ff.api.lib()
+
+        def fn():
+            if L.fft_griffin_lim(fc.handle, ic.handle, ff.api._fp(mag), F, H, 1, iters, 1, 7, ff.api._fp(re),
+                                 ff.api._fp(im)) != 1:
+                raise RuntimeError("fft_griffin_lim failed")
+        ola = (F - 1) * H + N
+        # per iteration: inverse (spectra in, frames out), overlap-add (frames
+        # in, signal out), projected STFT (signal and magnitudes in, spectra out)
+        nbytes = iters * (2 * F * bins * 4 + F * N * 4 + F * N * 4 + ola * 4 + ola * 4 + F * bins * 4
+                          + 2 * F * bins * 4)
     elif name == "stft_n1024_h256":
         L = 128 * 65536
         pcm = torch.rand(L, device="cuda", generator=g) * 2 - 1

@@ -539,6 +539,76 @@ static void run_complex_batch(FftContext* c, const float* in_re, const float* in
   finish_call(c, any_host);
 }
 
+// ------------------------------------------------------------------ Griffin-Lim steps
+// The two transforms of one Griffin-Lim iteration (phase_infer.hpp:140-197)
+// on device buffers, enqueued on the context's stream without host
+// synchronisation; the loop orders the two contexts' streams itself.
+namespace {
+struct AsyncScope {
+  FftContext* c;
+  bool was;
+  explicit AsyncScope(FftContext* ctx) : c(ctx), was(ctx->async) { c->async = true; }
+  ~AsyncScope() { c->async = was; }
+};
+}  // namespace
+
+size_t gl_inverse_enqueue(FftContext* c, const float* re, const float* im, size_t frames, float* frame_pcm) {
+  // fft_execute_complex_batched without recovery (fft_cffi.cpp:1042-1340)
+  if (c->N <= 0 || frames == 0) return 0;
+  std::lock_guard<std::recursive_mutex> lk(c->mu);
+  DeviceGuard g(c->device);
+  AsyncScope as(c);
+  run_complex_batch(c, re, im, frames, frame_pcm, nullptr);
+  return frames;
+}
+
+size_t gl_forward_project_enqueue(FftContext* c, const float* pcm, size_t pcm_len, int pad_mode,
+                                  size_t max_frames, const float* mag, float* re, float* im, int bins,
+                                  bool half, bool even_n, float* tr, float* ti, float* tm) {
+  // fft_execute_batched without recovery (fft_cffi.cpp:701-1034), then
+  // re + i im = mag e^{i arg} over the frames it produced
+  // (phase_infer.hpp:182-207)
+  const size_t frames = frame_count(c, pcm_len, pad_mode, max_frames);
+  if (frames == 0) return 0;
+  const int W = c->window ? c->window : c->N;
+  const int H = c->hop ? c->hop : W;
+  std::lock_guard<std::recursive_mutex> lk(c->mu);
+  DeviceGuard g(c->device);
+  const PostFlags pf = c->post_flags();
+  const size_t upd = std::min(frames, max_frames ? max_frames : frames);
+  if (c->bins() == bins && !pf.polar && !pf.reduce && single_pass(c->N, true) && is_device_ptr(pcm)) {
+    // one launch: the STFT's epilogue writes the projected spectra
+    StftArgs a{};
+    a.pcm = pcm;
+    a.pcm_len = (long long)std::min(pcm_len, (frames - 1) * (size_t)H + (size_t)W);
+    a.frames = (long long)upd;
+    a.N = c->N;
+    a.W = W;
+    a.H = H;
+    a.win = c->windows_enabled ? static_cast<const float*>(c->d_analysis.p) : nullptr;
+    a.mirror = stft_mirror(c) ? 1 : 0;
+    a.inverse = c->inverse ? 1 : 0;
+    a.pf = pf;
+    a.out_bins = bins;
+    a.out_stride = bins;
+    a.out_re = re;
+    a.out_im = im;
+    a.out_mag = tm;
+    a.mag_only = 4;
+    a.target = mag;
+    FFB_CHECK(launch_stft(a, c->logr_req, c->stream, &c->launches));
+    FFB_CHECK(cudaGetLastError());
+    return frames;
+  }
+  {
+    AsyncScope as(c);
+    run_stft(c, pcm, pcm_len, frames, W, H, true, c->bins(), true, pf, stft_mirror(c), tr, ti, tm);
+  }
+  FFB_CHECK(launch_gl_project(mag, tr, ti, re, im, (long long)(upd * (size_t)bins), bins, half ? 1 : 0,
+                              even_n ? 1 : 0, c->stream));
+  return frames;
+}
+
 }  // namespace ffb
 
 using namespace ffb;

@@ -101,4 +101,15 @@ FftContext* as_ctx(void* h);
 // (fft_cffi.cpp:163-208: kind, parameter p1, normalisation policy).
 std::vector<float> window_taps(int kind, int W, float p1, float p2, int norm_policy);
 
+// One Griffin-Lim iteration's transforms on device buffers, enqueued on the
+// context's stream with no host synchronisation (they throw on CUDA errors):
+// the inverse batch of (re, im) into frame_pcm, and the forward STFT of pcm
+// whose spectra are projected onto the magnitudes mag into (re, im) -- by
+// the STFT's own epilogue where the plan allows, else through (tr, ti, tm)
+// and a projection kernel.  Each returns the frames it produced, 0 if none.
+size_t gl_inverse_enqueue(FftContext* c, const float* re, const float* im, size_t frames, float* frame_pcm);
+size_t gl_forward_project_enqueue(FftContext* c, const float* pcm, size_t pcm_len, int pad_mode,
+                                  size_t max_frames, const float* mag, float* re, float* im, int bins,
+                                  bool half, bool even_n, float* tr, float* ti, float* tm);
+
 }  // namespace ffb

@@ -168,6 +168,23 @@ __device__ __forceinline__ float2 mag_phasor(float2 X, float* mag) {
   return unit_phasor(X, m);
 }
 
+// Griffin-Lim projection (phase_infer.hpp:190-196): the magnitude m with the
+// phase of X, m e^{i atan2(X.y, X.x)}, formed as m X / |X|.  X = 0 takes
+// atan2's phase of signed zeros: 0, or pi where X.x is -0 (cos = -1; the
+// sine's 8.7e-8 is left out).
+__device__ __forceinline__ float2 gl_project(float2 X, float m) {
+  const float s = __fmaf_rn(X.x, X.x, __fmul_rn(X.y, X.y));
+  float r;
+  if (s > 1e-36f && s < 1e36f) {
+    r = m * rsqrtf(s);
+  } else {
+    const float h = hypotf(X.x, X.y);
+    if (h == 0.f) return make_float2(signbit(X.x) ? -m : m, 0.f);
+    r = m / h;
+  }
+  return make_float2(X.x * r, X.y * r);
+}
+
 // Frame f of a (possibly multi-signal) STFT: its first sample and how many
 // samples it takes from the signal (fft_cffi.cpp:765-791: frame f covers
 // pcm[f*H .. f*H + W), zero beyond the signal end and from W up to N).
@@ -217,11 +234,25 @@ __device__ __forceinline__ void group_loss_partial(float v, int t, float* part) 
 // (forward half spectrum, magnitude array alone), 4 |X| into the magnitude
 // array and the unit phasor X / |X| into out_phasor (0 where |X| = 0), 5 the
 // residual |X| - target into the magnitude array, the unit phasor, and the
-// frame's sum of squared residuals (loss_part, loss_slots per frame).
+// frame's sum of squared residuals (loss_part, loss_slots per frame), 6 the
+// Griffin-Lim projection: mode 0's (re, im) replaced by target e^{i arg}
+// (target: the magnitudes, same layout as out_re; no magnitude array).
 template <int MODE>
 struct StftIO {
   StftArgs a;
   int logN;
+  // modes that write the magnitude array alone or with a phasor row
+  static constexpr bool kMagOnly = MODE >= 3 && MODE <= 5;
+  static constexpr bool kPhasor = MODE == 4 || MODE == 5;
+  // modes that read the target row (through the `mg` row pointer in mode 6)
+  static constexpr bool kTarget = MODE == 5 || MODE == 6;
+
+  // Row of the magnitude array at offset ob; in mode 6, the target's row
+  // (read, never written).
+  __device__ __forceinline__ float* mag_row(long long ob) const {
+    if constexpr (MODE == 6) return const_cast<float*>(a.target) + ob;
+    return a.out_mag + ob;
+  }
 
   template <class S>
   __device__ __forceinline__ void load(long long f, int t, float2 (&v)[S::R], float2*, const Twiddles&) const {
@@ -291,8 +322,8 @@ struct StftIO {
     const long long ob = f * a.out_stride;
     const bool mag_is_re = (MODE == 1) || (MODE == 2 && a.mag_from_real);
     emit(MODE == 4 ? reinterpret_cast<float*>(a.out_phasor + ob) : a.out_re + (MODE == 3 ? 0 : ob),
-         a.out_im + (MODE >= 3 ? 0 : ob), a.out_mag + ob, (int)k, X,
-         k == 0 || 2 * k == a.N, 1.0f / (float)a.N, mag_is_re);
+         a.out_im + (kMagOnly ? 0 : ob), mag_row(ob), (int)k, X, k == 0 || 2 * k == a.N,
+         1.0f / (float)a.N, mag_is_re);
   }
 
   // Bin k of the output: inverse scaling, exact-real DC / Nyquist, post
@@ -303,7 +334,14 @@ struct StftIO {
     // Real input: DC and Nyquist are exactly real (imag +0), as in the
     // reference's radix-2 executors.
     if (dc_or_nyq) X.y = 0.f;
-    if constexpr (MODE >= 3) {
+    if constexpr (MODE == 6) {
+      X = post_hook_m<0>(X, k, a.N, a.pf);
+      const float2 P = gl_project(X, mg[k]);  // mg: the target row
+      re[k] = P.x;
+      im[k] = P.y;
+      return;
+    }
+    if constexpr (kMagOnly) {
       const float m = cabs_fast(X.x, X.y);
       mg[k] = m;
       if constexpr (MODE == 4) reinterpret_cast<float2*>(re)[k] = unit_phasor(X, m);  // re: phasor row
@@ -319,12 +357,12 @@ struct StftIO {
   __device__ __forceinline__ void store(long long f, int t, float2 (&v)[S::R], float2* sm,
                                         const Twiddles& tw) const {
     constexpr int M = S::M, T = S::T, R = S::R;
-    // L2 loss: the frame's target row is fetched first, so that its loads
-    // are in flight across the tile exchange
-    float tgv[MODE == 5 ? R : 1];
+    // L2 loss and projection: the frame's target row (bins 0..M) is fetched
+    // first, so that its loads are in flight across the tile exchange
+    float tgv[kTarget ? R : 1];
     float tg_nyq = 0.f;
-    if constexpr (MODE == 5) {
-      const bool okf = f < a.frames;
+    if constexpr (kTarget) {
+      const bool okf = f < a.frames && a.out_bins == M + 1 && !a.inverse;
       const float* tg = a.target + (okf ? f : 0) * a.out_stride + t;
 #pragma unroll
       for (int i = 0; i < R; ++i) tgv[i] = okf ? __ldg(tg + i * T) : 0.f;
@@ -334,9 +372,9 @@ struct StftIO {
     GroupSync::sync<S>();
     if (f >= a.frames) return;
     const long long ob = f * a.out_stride;
-    float* re = (MODE >= 4) ? reinterpret_cast<float*>(a.out_phasor + ob) : a.out_re + (MODE == 3 ? 0 : ob);
-    float* im = a.out_im + (MODE >= 3 ? 0 : ob);
-    float* mg = a.out_mag + ob;
+    float* re = kPhasor ? reinterpret_cast<float*>(a.out_phasor + ob) : a.out_re + (MODE == 3 ? 0 : ob);
+    float* im = a.out_im + (kMagOnly ? 0 : ob);
+    float* mg = mag_row(ob);
     const bool mag_is_re = (MODE == 1) || (MODE == 2 && a.mag_from_real);
     if (a.N == 1) {
       if (t == 0) emit(re, im, mg, 0, make_float2(v[0].x, 0.f), true, 1.0f, mag_is_re);
@@ -374,6 +412,23 @@ struct StftIO {
           acc = __fmaf_rn(r, r, acc);
         }
         group_loss_partial<S>(acc, t, a.loss_part + f * loss_slots(M));
+        return;
+      }
+      if constexpr (MODE == 6) {
+#pragma unroll
+        for (int i = 0; i < R; ++i) {
+          const float2 zm = sm[pidx((M - t - i * T) & (M - 1))];
+          float2 X = untangle_bin(v[i], zm, w.half(i));
+          if ((i == 0 && t == 0) || a.pf.clear_imag) X.y = 0.f;  // DC is real
+          const float2 P = gl_project(X, tgv[i]);
+          pr[i * T] = P.x;
+          pi[i * T] = P.y;
+        }
+        if (t == 0) {  // Nyquist X[M] = Re Z[0] - Im Z[0]
+          const float2 P = gl_project(make_float2(v[0].x - v[0].y, 0.f), tg_nyq);
+          re[M] = P.x;
+          im[M] = P.y;
+        }
         return;
       }
 #pragma unroll

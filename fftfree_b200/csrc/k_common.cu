@@ -52,9 +52,11 @@ int choose_logr(int logm, int requested_log, bool real_path) {
 // ------------------------------------------------------------------ OLA
 // fft_cffi.cpp:1119-1146: out[t] = sum over frames f with f*H <= t < f*H + N
 // of frame_f[t - f*H], t < frames*N, accumulated in frame order; with COLA,
-// divided by the summed weights where that sum exceeds 1e-12.
+// divided by the summed weights where that sum exceeds 1e-12.  Griffin-Lim
+// asks for len = (frames-1)*H + N samples instead (phase_infer.hpp:147-168),
+// which exceeds frames*N when H > N; samples no frame covers are 0.
 __global__ void k_ola(OlaArgs a) {
-  const long long total = a.frames * (long long)a.N;
+  const long long total = a.len > 0 ? a.len : a.frames * (long long)a.N;
   for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < total;
        t += (long long)gridDim.x * blockDim.x) {
     long long fhi = t / a.H;
@@ -72,7 +74,7 @@ __global__ void k_ola(OlaArgs a) {
 }
 
 cudaError_t launch_ola(const OlaArgs& a, cudaStream_t s, uint64_t* launches) {
-  const long long total = a.frames * (long long)a.N;
+  const long long total = a.len > 0 ? a.len : a.frames * (long long)a.N;
   if (total <= 0) return cudaSuccess;
   long long blocks = (total + 255) / 256;
   if (blocks > 148 * 64) blocks = 148 * 64;
@@ -110,6 +112,27 @@ cudaError_t launch_gl_project(const float* mag, const float* tr, const float* ti
   long long blocks = (nbins + 255) / 256;
   if (blocks > 148 * 32) blocks = 148 * 32;
   k_gl_project<<<(unsigned)blocks, 256, 0, s>>>(mag, tr, ti, re, im, nbins, bins, half, even_n);
+  return cudaGetLastError();
+}
+
+// phase_infer.hpp:133-137: out = magnitude * (cos, sin) of the initial phase,
+// the float products of the reference.
+__global__ void k_gl_init(const float* __restrict__ mag, const float2* __restrict__ cs, float* __restrict__ re,
+                          float* __restrict__ im, long long n) {
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x) {
+    const float m = __ldg(mag + i);
+    const float2 u = __ldg(cs + i);
+    re[i] = __fmul_rn(m, u.x);
+    im[i] = __fmul_rn(m, u.y);
+  }
+}
+
+cudaError_t launch_gl_init(const float* mag, const float2* cs, float* re, float* im, long long n, cudaStream_t s) {
+  if (n <= 0) return cudaSuccess;
+  long long blocks = (n + 255) / 256;
+  if (blocks > 148 * 32) blocks = 148 * 32;
+  k_gl_init<<<(unsigned)blocks, 256, 0, s>>>(mag, cs, re, im, n);
   return cudaGetLastError();
 }
 

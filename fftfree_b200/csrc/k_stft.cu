@@ -7,6 +7,10 @@ cudaError_t launch_stft(const StftArgs& a, int req_logr, cudaStream_t s, uint64_
   const int logm = (a.N == 1) ? 0 : ilog2i(a.N) - 1;
   const int logr = choose_logr(logm, req_logr, true);
   if (logr < 0) return cudaErrorInvalidValue;
+  if (a.mag_only == 4) {
+    if (post_mode(a.pf) != 0) return cudaErrorInvalidValue;
+    return dispatch(StftIO<6>{a, ilog2i(a.N)}, logm, logr, a.frames, s, launches);
+  }
   if (a.mag_only == 3) return dispatch(StftIO<5>{a, ilog2i(a.N)}, logm, logr, a.frames, s, launches);
   if (a.mag_only == 2) return dispatch(StftIO<4>{a, ilog2i(a.N)}, logm, logr, a.frames, s, launches);
   if (a.mag_only) return dispatch(StftIO<3>{a, ilog2i(a.N)}, logm, logr, a.frames, s, launches);

@@ -40,10 +40,12 @@ struct StftArgs {
   // forward R2C half spectrum, bins 0..N/2: 1 = only |X| (out_mag),
   // 2 = |X| (out_mag) and the unit phasor X / |X| (out_phasor, 0 where |X| = 0),
   // 3 = the residual |X| - target (out_mag), the phasor, and per-warp sums of
-  // the squared residuals (loss_part)
+  // the squared residuals (loss_part); 4 = the Griffin-Lim projection
+  // target e^{i arg X} into (out_re, out_im), no magnitude array (any
+  // spectrum layout; post flags without polar or reduce)
   int mag_only;
   float2* out_phasor;
-  const float* target;  // mag_only 3: same layout as out_mag
+  const float* target;  // mag_only 3 and 4: same layout as the outputs
   float* loss_part;     // mag_only 3: stft_loss_parts(frames, N) floats
 };
 // Partial sums of the squared residual an L2-loss launch writes.
@@ -105,7 +107,8 @@ struct OlaArgs {
   int N, H;
   int cola;
   const float* weight;  // device, N entries (analysis*synthesis) or nullptr (=1)
-  float* out;           // frames * N samples
+  float* out;           // `len` samples
+  long long len;        // samples written; 0: frames * N
 };
 
 // Twiddle pyramid (levels 0..max_log) on the current device.
@@ -147,6 +150,9 @@ cudaError_t launch_cplx_batch(const CplxBatchArgs& a, int logr, cudaStream_t s, 
 cudaError_t launch_ola(const OlaArgs& a, cudaStream_t s, uint64_t* launches);
 // Griffin-Lim projection: re + i im = mag e^{i atan2(ti, tr)} (half spectrum:
 // DC and, for even N, Nyquist imaginary parts cleared).
+// Griffin-Lim initial spectra: re = mag * cs.x, im = mag * cs.y (cs: the
+// cosines and sines of the initial phases).
+cudaError_t launch_gl_init(const float* mag, const float2* cs, float* re, float* im, long long n, cudaStream_t s);
 cudaError_t launch_gl_project(const float* mag, const float* tr, const float* ti, float* re, float* im,
                               long long nbins, int bins, int half, int even_n, cudaStream_t s);
 // Streaming ISTFT step (fft_cffi.cpp:1597-1742): F inverse frames of N

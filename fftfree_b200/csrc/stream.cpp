@@ -6,10 +6,12 @@
 
 #include <algorithm>
 #include <cmath>
+#include <cstdint>
 #include <cstdio>
 #include <cstdlib>
 #include <random>
 #include <stdexcept>
+#include <thread>
 #include <vector>
 
 #include "../../include/fft_cffi.h"
@@ -19,6 +21,92 @@
 
 namespace ffb {
 namespace {
+
+// fn(lo, hi) over [0, n) split into contiguous ranges, one per host thread
+// (up to 16); small n on the calling thread alone.
+template <class Fn>
+void parallel_ranges(size_t n, Fn&& fn) {
+  const size_t kMinPerThread = 1 << 15;
+  size_t t = std::thread::hardware_concurrency();
+  t = std::max<size_t>(1, std::min<size_t>({t, 16, n / kMinPerThread}));
+  if (t <= 1) {
+    fn(size_t(0), n);
+    return;
+  }
+  std::vector<std::thread> pool;
+  pool.reserve(t - 1);
+  const size_t per = (n + t - 1) / t;
+  for (size_t k = 1; k < t; ++k) {
+    const size_t lo = std::min(n, k * per), hi = std::min(n, lo + per);
+    pool.emplace_back([&fn, lo, hi] { fn(lo, hi); });
+  }
+  fn(size_t(0), std::min(n, per));
+  for (std::thread& th : pool) th.join();
+}
+
+// Angle i of the n initial Griffin-Lim phases, as phase_infer.hpp:128-135
+// draws them: std::uniform_real_distribution<float>(-pi, pi) over
+// std::mt19937(seed), one 32-bit draw per angle (libstdc++'s
+// generate_canonical<float, 24>: u = float(x) / 2^32, 1 - 2^-24 where that
+// rounds to 1, then u * (b - a) + a in float).
+inline float gl_angle(uint32_t x) {
+  const float a = -3.14159265358979323846f, b = 3.14159265358979323846f;
+  float u = (float)x / 4294967296.0f;
+  if (u >= 1.0f) u = std::nextafter(1.0f, 0.0f);
+  return u * (b - a) + a;
+}
+
+// MT19937 tempering of a state word (Matsumoto and Nishimura, 1998).
+inline uint32_t mt_temper(uint32_t y) {
+  y ^= y >> 11;
+  y ^= (y << 7) & 0x9d2c5680u;
+  y ^= (y << 15) & 0xefc60000u;
+  return y ^ (y >> 18);
+}
+
+// out[i] = (cos, sin) of angle i (std::cos / std::sin of the float angle).
+// The generator's state recurrence
+//   x[k+624] = x[k+397] ^ (y >> 1) ^ (y odd ? 0x9908b0df : 0),
+//   y = (x[k] & 0x80000000) | (x[k+1] & 0x7fffffff),
+// with x[0..623] the standard seeding, runs sequentially over one array;
+// draw j is temper(x[624 + j]), and the tempering, the conversion and the
+// cosines and sines run on several host threads.  The first draws are
+// checked against std::mt19937 and std::uniform_real_distribution
+// themselves; on a mismatch every angle comes from them.
+void gl_initial_phasors(uint32_t seed, size_t n, float2* out) {
+  if (n == 0) return;
+  std::vector<uint32_t> x(n + 624);
+  x[0] = seed;
+  for (uint32_t i = 1; i < 624; ++i) x[i] = 1812433253u * (x[i - 1] ^ (x[i - 1] >> 30)) + i;
+  for (size_t k = 0; k < n; ++k) {
+    const uint32_t y = (x[k] & 0x80000000u) | (x[k + 1] & 0x7fffffffu);
+    x[k + 624] = x[k + 397] ^ (y >> 1) ^ ((y & 1u) ? 0x9908b0dfu : 0u);
+  }
+  const float kPi = 3.14159265358979323846f;
+  std::mt19937 rng(seed);
+  std::uniform_real_distribution<float> dist(-kPi, kPi);
+  bool same = true;
+  const size_t check = std::min<size_t>(n, 2 * 624 + 16);
+  for (size_t j = 0; j < check && same; ++j) same = dist(rng) == gl_angle(mt_temper(x[624 + j]));
+  if (!same) {
+    std::mt19937 r2(seed);
+    std::uniform_real_distribution<float> d2(-kPi, kPi);
+    for (size_t j = 0; j < n; ++j) out[j].x = d2(r2);
+    parallel_ranges(n, [&](size_t lo, size_t hi) {
+      for (size_t j = lo; j < hi; ++j) {
+        const float ang = out[j].x;
+        out[j] = make_float2(std::cos(ang), std::sin(ang));
+      }
+    });
+    return;
+  }
+  parallel_ranges(n, [&](size_t lo, size_t hi) {
+    for (size_t j = lo; j < hi; ++j) {
+      const float ang = gl_angle(mt_temper(x[624 + j]));
+      out[j] = make_float2(std::cos(ang), std::sin(ang));
+    }
+  });
+}
 
 bool verbose() {
   static const bool v = [] {
@@ -441,31 +529,17 @@ FFT_CFFI_API int fft_griffin_lim(void* ctx_forward, void* ctx_inverse, const flo
     const size_t ola_len = (frames - 1) * hp + plan_n;
     const int iters = (iterations > 0) ? iterations : 32;
     // Initial phases as the reference draws them (phase_infer.hpp:128-138):
-    // std::mt19937 and a float uniform in [-pi, pi), on the host.
-    const float kPi = 3.14159265358979323846f;
-    std::mt19937 rng(seed ? seed : 0x47d7bfad);
-    std::uniform_real_distribution<float> dist(-kPi, kPi);
-    // A device-resident magnitude is read back once for the initial spectra.
-    std::vector<float> mag_host;
-    const float* hmag = in_mag;
-    cudaPointerAttributes pa{};
-    if (cudaPointerGetAttributes(&pa, in_mag) == cudaSuccess && pa.type == cudaMemoryTypeDevice) {
-      mag_host.resize(total_bins);
-      if (cudaMemcpy(mag_host.data(), in_mag, total_bins * sizeof(float), cudaMemcpyDeviceToHost) != cudaSuccess)
-        return 0;
-      hmag = mag_host.data();
-    } else {
-      cudaGetLastError();
-    }
-    std::vector<float> re0(total_bins), im0(total_bins);
-    for (size_t i = 0; i < total_bins; ++i) {
-      const float a = dist(rng);
-      re0[i] = hmag[i] * std::cos(a);
-      im0[i] = hmag[i] * std::sin(a);
-    }
+    // std::mt19937 and a float uniform in [-pi, pi), in order on the host.
+    // Their cosines and sines (std::cos / std::sin of the float angle, as
+    // there) are evaluated by several host threads; the device multiplies
+    // them by the magnitudes.
+    std::vector<float2> cs(total_bins);
+    gl_initial_phasors(seed ? seed : 0x47d7bfad, total_bins, cs.data());
     // The iterations run on the device (phase_infer.hpp:140-208): the inverse
-    // batch, the count-normalised overlap-add, the forward STFT and the phase
-    // projection, with every intermediate in device memory.
+    // batch, the count-normalised overlap-add, and the forward STFT whose
+    // epilogue projects its spectra onto the target magnitudes, all enqueued
+    // without host synchronisation; the two contexts' streams are ordered by
+    // events when they differ.
     int prev = -1;
     cudaGetDevice(&prev);
     if (prev != fc->device) cudaSetDevice(fc->device);
@@ -475,61 +549,78 @@ FFT_CFFI_API int fft_griffin_lim(void* ctx_forward, void* ctx_inverse, const flo
         if (dev >= 0) cudaSetDevice(dev);
       }
     } restore{prev != fc->device ? prev : -1};
-    DevBuf d_mag, d_re, d_im, d_frames, d_ola, d_tr, d_ti, d_tm;
+    DevBuf d_spec, d_frames, d_ola, d_tmp;
     const size_t fb = total_bins * sizeof(float);
-    float* mag = static_cast<float*>(d_mag.get(fb));
-    float* re = static_cast<float*>(d_re.get(fb));
-    float* im = static_cast<float*>(d_im.get(fb));
-    float* tr = static_cast<float*>(d_tr.get(fb));
-    float* ti = static_cast<float*>(d_ti.get(fb));
-    float* tm = static_cast<float*>(d_tm.get(fb));
+    float* mag = static_cast<float*>(d_spec.get(3 * fb));
+    float* re = mag + total_bins;
+    float* im = re + total_bins;
+    // forward outputs of the unfused projection; first the cosines and sines
+    float* tr = static_cast<float*>(d_tmp.get(3 * fb));
+    float* ti = tr + total_bins;
+    float* tm = ti + total_bins;
     float* frame_pcm = static_cast<float*>(d_frames.get(frames * plan_n * sizeof(float)));
-    const size_t ola_cap = std::max(ola_len, frames * plan_n);
-    float* ola = static_cast<float*>(d_ola.get(ola_cap * sizeof(float)));
+    float* ola = static_cast<float*>(d_ola.get(ola_len * sizeof(float)));
     cudaStream_t st = fc->stream;
+    cudaStream_t ist = ic->stream;
     auto ok = [](cudaError_t e) {
       if (e != cudaSuccess) throw std::runtime_error("cuda");
     };
+    struct Events {
+      cudaEvent_t inv = nullptr, fwd = nullptr;
+      ~Events() {
+        if (inv) cudaEventDestroy(inv);
+        if (fwd) cudaEventDestroy(fwd);
+      }
+    } ev;
+    const bool two = ist != st;
+    if (two) {
+      ok(cudaEventCreateWithFlags(&ev.inv, cudaEventDisableTiming));
+      ok(cudaEventCreateWithFlags(&ev.fwd, cudaEventDisableTiming));
+    }
     ok(cudaMemcpyAsync(mag, in_mag, fb, cudaMemcpyDefault, st));
-    ok(cudaMemcpyAsync(re, re0.data(), fb, cudaMemcpyHostToDevice, st));
-    ok(cudaMemcpyAsync(im, im0.data(), fb, cudaMemcpyHostToDevice, st));
+    ok(cudaMemcpyAsync(tr, cs.data(), 2 * fb, cudaMemcpyHostToDevice, st));
+    ok(launch_gl_init(mag, reinterpret_cast<const float2*>(tr), re, im, (long long)total_bins, st));
     ok(cudaStreamSynchronize(st));
     // The reference refines out_real/out_imag in place, so a failed pass
     // leaves the spectra of the last completed one there.
     auto flush = [&]() {
+      if (two) ok(cudaStreamSynchronize(ist));
       ok(cudaMemcpyAsync(out_real, re, fb, cudaMemcpyDefault, st));
       ok(cudaMemcpyAsync(out_imag, im, fb, cudaMemcpyDefault, st));
       ok(cudaStreamSynchronize(st));
     };
+    OlaArgs o{};
+    o.frames_buf = frame_pcm;
+    o.frames = (long long)frames;
+    o.N = (int)plan_n;
+    o.H = (int)hp;
+    o.cola = 1;  // divide by the number of frames covering the sample
+    o.weight = nullptr;
+    o.out = ola;
+    o.len = (long long)ola_len;  // every sample written: no clearing
     for (int it = 0; it < iters; ++it) {
-      const size_t pr = fft_execute_complex_batched(ctx_inverse, re, im, frames, frame_pcm, pad_mode, 0, frames);
-      if (pr == 0) {
+      size_t pr = 0, ff = 0;
+      try {
+        if (two && it > 0) ok(cudaStreamWaitEvent(ist, ev.fwd, 0));
+        pr = gl_inverse_enqueue(ic, re, im, frames, frame_pcm);
+        if (pr != 0) {
+          if (two) {
+            ok(cudaEventRecord(ev.inv, ist));
+            ok(cudaStreamWaitEvent(st, ev.inv, 0));
+          }
+          o.frames = (long long)std::min(pr, frames);
+          ok(launch_ola(o, st, &fc->launches));
+          ff = gl_forward_project_enqueue(fc, ola, ola_len, pad_mode, frames, mag, re, im, (int)bins, half,
+                                          (plan_n & 1) == 0, tr, ti, tm);
+          if (two) ok(cudaEventRecord(ev.fwd, st));
+        }
+      } catch (...) {
+        pr = 0;
+      }
+      if (pr == 0 || ff == 0) {
         flush();
         return 0;
       }
-      ok(cudaStreamSynchronize(ic->stream));
-      const size_t uf = std::min(pr, frames);
-      ok(cudaMemsetAsync(ola, 0, ola_cap * sizeof(float), st));
-      OlaArgs o{};
-      o.frames_buf = frame_pcm;
-      o.frames = (long long)uf;
-      o.N = (int)plan_n;
-      o.H = (int)hp;
-      o.cola = 1;  // divide by the number of frames covering the sample
-      o.weight = nullptr;
-      o.out = ola;
-      ok(launch_ola(o, st, &fc->launches));
-      ok(cudaStreamSynchronize(st));
-      const size_t ff = fft_execute_batched(ctx_forward, ola, ola_len, tr, ti, tm, pad_mode, 0, frames);
-      if (ff == 0) {
-        flush();
-        return 0;
-      }
-      ok(cudaStreamSynchronize(fc->stream));
-      const size_t uff = std::min(ff, frames);
-      ok(launch_gl_project(mag, tr, ti, re, im, (long long)(uff * bins), (int)bins, half ? 1 : 0,
-                           (plan_n & 1) == 0 ? 1 : 0, st));
-      ok(cudaStreamSynchronize(st));
     }
     flush();
     return 1;

@@ -55,6 +55,85 @@ def test_griffin_lim_matches_oracle(N, H, frames, iters):
     assert np.all(im[:, 0] == 0) and np.all(im[:, -1] == 0)
 
 
+def _gl_case(N, H, frames, iters, half=True, fwd_extra=None, seed=5):
+    """GPU and oracle Griffin-Lim on the STFT magnitudes of a test signal."""
+    fk = ctx_kwargs(N, transform=1, half_spectrum=1 if half else 0, window=N, hop=H, apply_windows=1,
+                    analysis_kind=1, **(fwd_extra or {}))
+    ik = ctx_kwargs(N, inverse=1, transform=2, half_spectrum=1 if half else 0, window=N, hop=H)
+    fc, ic = api.FftContext.full_v2(**fk), api.FftContext.full_v2(**ik)
+    fo, io = oracle_for(fk), oracle_for(ik)
+    plain = oracle_for(ctx_kwargs(N, transform=1, half_spectrum=1 if half else 0, window=N, hop=H,
+                                  apply_windows=1, analysis_kind=1))
+    x = _signal(frames, H, N, N + iters + H)
+    n, _, _, mag = plain.execute_batched(x, pad_mode=1, max_frames=frames)
+    assert n == frames
+    bins = mag.shape[-1]
+    re = np.zeros(frames * bins, np.float32)
+    im = np.zeros(frames * bins, np.float32)
+    return fc, ic, fo, io, np.ascontiguousarray(mag), re, im
+
+
+def _run_gl(fc, ic, mag, frames, H, half, iters, seed, re, im):
+    return api.lib().fft_griffin_lim(fc.handle, ic.handle, _fp(mag), frames, H, 1 if half else 0, iters, 1, seed,
+                                     _fp(re), _fp(im))
+
+
+@pytest.mark.parametrize("N,H,frames,iters", [(64, 80, 10, 3), (128, 128, 9, 2), (256, 300, 6, 2)])
+def test_griffin_lim_hop_at_or_beyond_frame(N, H, frames, iters):
+    # H > N leaves samples no frame covers: the overlap-add runs over the
+    # (frames-1)*H + N samples of the reference, zero in the gaps.
+    fc, ic, fo, io, mag, re, im = _gl_case(N, H, frames, iters)
+    assert _run_gl(fc, ic, mag, frames, H, True, iters, 11, re, im) == 1
+    rok, rre, rim = sg.griffin_lim(fo, io, mag, frames, H, True, iters, 1, 11)
+    assert rok == 1
+    assert_close(re + 1j * im, (rre + 1j * rim).reshape(-1), 4 * iters * tol_for(N), "griffin-lim spectrum")
+
+
+@pytest.mark.parametrize("N,H,frames,iters", [(256, 64, 12, 3), (64, 16, 20, 2)])
+def test_griffin_lim_full_spectrum(N, H, frames, iters):
+    # full-spectrum contexts: the projection runs in the STFT's general
+    # (two-sided) epilogue
+    fc, ic, fo, io, mag, re, im = _gl_case(N, H, frames, iters, half=False)
+    assert mag.shape[-1] == N
+    assert _run_gl(fc, ic, mag, frames, H, False, iters, 3, re, im) == 1
+    rok, rre, rim = sg.griffin_lim(fo, io, mag, frames, H, False, iters, 1, 3)
+    assert rok == 1
+    assert_close(re + 1j * im, (rre + 1j * rim).reshape(-1), 4 * iters * tol_for(N), "griffin-lim spectrum")
+
+
+@pytest.mark.parametrize("extra", [dict(store_polar=1), dict(reduce_magnitude=1)])
+def test_griffin_lim_polar_forward_context(extra):
+    # A forward context that stores polar values or magnitudes: the
+    # projection reads its (re, im) outputs as the reference does, through
+    # the separate projection kernel.
+    N, H, frames, iters = 128, 32, 14, 2
+    fc, ic, fo, io, mag, re, im = _gl_case(N, H, frames, iters, fwd_extra=extra)
+    assert _run_gl(fc, ic, mag, frames, H, True, iters, 9, re, im) == 1
+    rok, rre, rim = sg.griffin_lim(fo, io, mag, frames, H, True, iters, 1, 9)
+    assert rok == 1
+    # atan2 of (|X|, arg X) amplifies rounding near the branch cut less than
+    # a spectrum would; compare as the other cases do
+    assert_close(re + 1j * im, (rre + 1j * rim).reshape(-1), 4 * iters * tol_for(N), "griffin-lim spectrum")
+
+
+def test_griffin_lim_contexts_on_one_stream():
+    # both contexts on one caller stream: no cross-stream events, same result
+    N, H, frames, iters = 256, 64, 16, 4
+    fc, ic, fo, io, mag, re, im = _gl_case(N, H, frames, iters)
+    assert _run_gl(fc, ic, mag, frames, H, True, iters, 7, re, im) == 1
+    s = torch.cuda.Stream()
+    fc.set_stream(s.cuda_stream)
+    ic.set_stream(s.cuda_stream)
+    re2, im2 = np.zeros_like(re), np.zeros_like(im)
+    assert _run_gl(fc, ic, mag, frames, H, True, iters, 7, re2, im2) == 1
+    assert np.array_equal(re, re2) and np.array_equal(im, im2)
+    fc.set_stream(0)
+    ic.set_stream(0)
+    re3, im3 = np.zeros_like(re), np.zeros_like(im)
+    assert _run_gl(fc, ic, mag, frames, H, True, iters, 7, re3, im3) == 1
+    assert np.array_equal(re, re3) and np.array_equal(im, im3)
+
+
 def test_griffin_lim_converges_and_device_magnitude():
     N, H, frames = 512, 128, 32
     fc, ic, fo, io = _gl_pair(N, H)
