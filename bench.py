@@ -578,10 +578,85 @@ def measure_legs(ff, torch, stream, reps: int = 10):
     c0.close()
     c1.close()
     del x2, y2
+    legs["griffin_lim_n1024_h256_f4096"] = measure_griffin_lim(ff, torch)
     legs["autograd_stft_magnitude"] = measure_autograd(torch, stream, timed)
     legs["ragged_r2c_4096"] = measure_ragged(ff, torch, stream, timed)
     legs["precision_c2c_n65536_b2048"] = measure_precision(ff, torch, stream, timed)
     return legs
+
+
+def measure_griffin_lim(ff, torch, reps: int = 5):
+    """fft_griffin_lim (fft_cffi.cpp:2176-2248) on 4096 frames x 513 bins
+    (N=W=1024, H=256, Hann analysis), device magnitudes and outputs: host
+    wall clock per synchronous call at 32 iterations, and the per-iteration
+    cost from the 32- and 96-iteration calls.  Beside it the reference's own
+    Griffin-Lim (oracle/_ref release build, host buffers, all host cores up
+    to 16) on the same shape at 2 and 4 iterations."""
+    import numpy as np
+    N, H, F = 1024, 256, 4096
+    bins = N // 2 + 1
+    g = torch.Generator(device="cuda").manual_seed(5)
+    mag = torch.rand(F * bins, device="cuda", generator=g)
+    re, im = torch.empty_like(mag), torch.empty_like(mag)
+    fc = ff.FftContext.full_v2(N, kernel=2, window=N, hop=H, transform=1, half_spectrum=1, apply_windows=1,
+                               analysis_kind=1)
+    ic = ff.FftContext.full_v2(N, kernel=2, inverse=1, transform=2, half_spectrum=1, window=N, hop=H)
+    L = ff.api.lib()
+
+    def call_ms(iters):
+        ts = []
+        for _ in range(reps):
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            if L.fft_griffin_lim(fc.handle, ic.handle, ff.api._fp(mag), F, H, 1, iters, 1, 7, ff.api._fp(re),
+                                 ff.api._fp(im)) != 1:
+                raise RuntimeError("fft_griffin_lim failed")
+            torch.cuda.synchronize()
+            ts.append((time.perf_counter() - t0) * 1e3)
+        return statistics.median(ts)
+
+    call_ms(2)
+    ms32, ms96 = call_ms(32), call_ms(96)
+    leg = {"frames": F, "bins": bins, "iterations": 32, "ms_per_call": round(ms32, 3),
+           "us_per_iteration": round((ms96 - ms32) / 64 * 1e3, 2),
+           "setup_ms": round(ms32 - 32 * (ms96 - ms32) / 64, 3)}
+    fc.close()
+    ic.close()
+    try:
+        from oracle import reflib
+        if os.path.exists(reflib.release_path()):
+            RL = reflib.release_lib()
+            th = max(1, min(16, os.cpu_count() or 1))
+            base = dict(n=N, threads=th, lanes=1, inverse=0, kernel=2, radix=0, radix_pattern=None, pad_mode=1,
+                        window=N, hop=H, transform=1, reduce_magnitude=0, store_polar=0, half_spectrum=1,
+                        allow_outer_parallel=1, allow_inner_parallel=0, inner_threads=0, save_crash_logs=0,
+                        silent_crash_reports=1, apply_windows=0, apply_ola=0, analysis_kind=0, analysis_p1=0.0,
+                        analysis_p2=0.0, synthesis_kind=0, synthesis_p1=0.0, synthesis_p2=0.0, norm_policy=0,
+                        cola_mode=0)
+            fk = dict(base, apply_windows=1, analysis_kind=1)
+            ik = dict(base, inverse=1, transform=2)
+            rf, ri = reflib.RefContext.full_v2(RL, **fk), reflib.RefContext.full_v2(RL, **ik)
+            hm = mag.cpu().numpy()
+            hr, hi = np.zeros_like(hm), np.zeros_like(hm)
+
+            def ref_ms(iters):
+                t0 = time.perf_counter()
+                if RL.fft_griffin_lim(rf.h, ri.h, reflib.fp(hm), F, H, 1, iters, 1, 7, reflib.fp(hr),
+                                      reflib.fp(hi)) != 1:
+                    raise RuntimeError("reference fft_griffin_lim failed")
+                return (time.perf_counter() - t0) * 1e3
+
+            r2, r4 = ref_ms(2), ref_ms(4)
+            per = (r4 - r2) / 2
+            leg["cpu_baseline"] = {"kind": "reference", "threads": th, "ms_per_iteration": round(per, 2),
+                                    "setup_ms": round(r2 - 2 * per, 2),
+                                    "ms_per_call_32_iterations_projected": round(r2 + 30 * per, 1),
+                                    "sample": "2- and 4-iteration calls, same shape and magnitudes"}
+            rf.close()
+            ri.close()
+    except Exception as e:  # the GPU figures stand without the reference beside them
+        leg["cpu_baseline"] = {"unavailable": str(e)[:200]}
+    return leg
 
 
 def measure_precision(ff, torch, stream, timed):

@@ -836,6 +836,11 @@ FFT_CFFI_API void fft_free(void* handle) {
     c->d_t2d.release();
     c->d_tma_timeouts.release();
     if (c->h_tma_timeouts) cudaFreeHost(c->h_tma_timeouts);
+    c->d_gl_spec.release();
+    c->d_gl_frames.release();
+    c->d_gl_ola.release();
+    c->d_gl_tmp.release();
+    if (c->h_gl_cs) cudaFreeHost(c->h_gl_cs);
     for (cudaStream_t st : {c->up_stream, c->down_stream})
       if (st) {
         cudaStreamSynchronize(st);

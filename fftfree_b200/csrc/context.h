@@ -65,6 +65,14 @@ struct FftContext {
   DevBuf d_queue, d_queue2;
   size_t q_off = 0, q_end = 0;
   DevBuf d_sre, d_sim, d_smg;  // push_pcm outputs the caller leaves NULL
+  // Griffin-Lim working set, kept on the forward context between calls:
+  // magnitudes and spectra, the inverse's frames, the overlap-added signal,
+  // the unfused forward outputs; the generator's state words and the
+  // initial phasors in pinned host memory
+  DevBuf d_gl_spec, d_gl_frames, d_gl_ola, d_gl_tmp;
+  std::vector<uint32_t> h_gl_state;
+  float2* h_gl_cs = nullptr;
+  size_t h_gl_cs_cap = 0;
 
   // --- device state ---
   int device = 0;

@@ -5,6 +5,8 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
+#include <chrono>
 #include <cmath>
 #include <cstdint>
 #include <cstdio>
@@ -64,48 +66,87 @@ inline uint32_t mt_temper(uint32_t y) {
   return y ^ (y >> 18);
 }
 
-// out[i] = (cos, sin) of angle i (std::cos / std::sin of the float angle).
-// The generator's state recurrence
+// The n initial phasors (cos, sin) of the angles above into the pinned host
+// array out[], each block of them copied on to dev[] on stream s as soon as
+// it is complete (std::cos / std::sin of the float angle).  The generator's
+// state recurrence
 //   x[k+624] = x[k+397] ^ (y >> 1) ^ (y odd ? 0x9908b0df : 0),
 //   y = (x[k] & 0x80000000) | (x[k+1] & 0x7fffffff),
-// with x[0..623] the standard seeding, runs sequentially over one array;
-// draw j is temper(x[624 + j]), and the tempering, the conversion and the
-// cosines and sines run on several host threads.  The first draws are
-// checked against std::mt19937 and std::uniform_real_distribution
-// themselves; on a mismatch every angle comes from them.
-void gl_initial_phasors(uint32_t seed, size_t n, float2* out) {
-  if (n == 0) return;
-  std::vector<uint32_t> x(n + 624);
-  x[0] = seed;
-  for (uint32_t i = 1; i < 624; ++i) x[i] = 1812433253u * (x[i - 1] ^ (x[i - 1] >> 30)) + i;
-  for (size_t k = 0; k < n; ++k) {
-    const uint32_t y = (x[k] & 0x80000000u) | (x[k + 1] & 0x7fffffffu);
-    x[k + 624] = x[k + 397] ^ (y >> 1) ^ ((y & 1u) ? 0x9908b0dfu : 0u);
-  }
+// with x[0..623] the standard seeding, runs sequentially over one array (x,
+// kept by the caller between calls) on the calling thread; draw j is
+// temper(x[624 + j]).  The tempering, the conversion, the cosines and sines
+// and the copies of each block run on worker threads as the recurrence
+// passes the block's end.  The first draws are checked against std::mt19937
+// and std::uniform_real_distribution themselves; on a mismatch every angle
+// comes from them.  Returns false if a copy could not be enqueued.
+bool gl_initial_phasors(uint32_t seed, size_t n, std::vector<uint32_t>& x, float2* out, float2* dev,
+                        int device, cudaStream_t s) {
+  if (n == 0) return true;
+  if (x.size() < n + 624) x.resize(n + 624);
+  uint32_t* xs = x.data();
+  xs[0] = seed;
+  for (uint32_t i = 1; i < 624; ++i) xs[i] = 1812433253u * (xs[i - 1] ^ (xs[i - 1] >> 30)) + i;
+  auto recur = [xs](size_t k0, size_t k1) {
+    for (size_t k = k0; k < k1; ++k) {
+      const uint32_t y = (xs[k] & 0x80000000u) | (xs[k + 1] & 0x7fffffffu);
+      xs[k + 624] = xs[k + 397] ^ (y >> 1) ^ ((y & 1u) ? 0x9908b0dfu : 0u);
+    }
+  };
   const float kPi = 3.14159265358979323846f;
-  std::mt19937 rng(seed);
-  std::uniform_real_distribution<float> dist(-kPi, kPi);
-  bool same = true;
   const size_t check = std::min<size_t>(n, 2 * 624 + 16);
-  for (size_t j = 0; j < check && same; ++j) same = dist(rng) == gl_angle(mt_temper(x[624 + j]));
-  if (!same) {
-    std::mt19937 r2(seed);
-    std::uniform_real_distribution<float> d2(-kPi, kPi);
-    for (size_t j = 0; j < n; ++j) out[j].x = d2(r2);
-    parallel_ranges(n, [&](size_t lo, size_t hi) {
+  recur(0, check);
+  {
+    std::mt19937 rng(seed);
+    std::uniform_real_distribution<float> dist(-kPi, kPi);
+    bool same = true;
+    for (size_t j = 0; j < check && same; ++j) same = dist(rng) == gl_angle(mt_temper(xs[624 + j]));
+    if (!same) {
+      std::mt19937 r2(seed);
+      std::uniform_real_distribution<float> d2(-kPi, kPi);
+      for (size_t j = 0; j < n; ++j) out[j].x = d2(r2);
+      parallel_ranges(n, [&](size_t lo, size_t hi) {
+        for (size_t j = lo; j < hi; ++j) {
+          const float ang = out[j].x;
+          out[j] = make_float2(std::cos(ang), std::sin(ang));
+        }
+      });
+      return cudaMemcpyAsync(dev, out, n * sizeof(float2), cudaMemcpyHostToDevice, s) == cudaSuccess;
+    }
+  }
+  const size_t kBlock = size_t(1) << 16;
+  const size_t blocks = (n + kBlock - 1) / kBlock;
+  std::atomic<size_t> produced{check}, next{0};
+  std::atomic<bool> failed{false};
+  auto work = [&](bool wait) {
+    if (wait && cudaSetDevice(device) != cudaSuccess) failed = true;
+    for (;;) {
+      const size_t b = next.fetch_add(1);
+      if (b >= blocks) return;
+      const size_t lo = b * kBlock, hi = std::min(n, lo + kBlock);
+      // the calling thread produces every block before it takes one
+      while (wait && produced.load(std::memory_order_acquire) < hi) std::this_thread::yield();
       for (size_t j = lo; j < hi; ++j) {
-        const float ang = out[j].x;
+        const float ang = gl_angle(mt_temper(xs[624 + j]));
         out[j] = make_float2(std::cos(ang), std::sin(ang));
       }
-    });
-    return;
-  }
-  parallel_ranges(n, [&](size_t lo, size_t hi) {
-    for (size_t j = lo; j < hi; ++j) {
-      const float ang = gl_angle(mt_temper(x[624 + j]));
-      out[j] = make_float2(std::cos(ang), std::sin(ang));
+      if (cudaMemcpyAsync(dev + lo, out + lo, (hi - lo) * sizeof(float2), cudaMemcpyHostToDevice, s) !=
+          cudaSuccess)
+        failed = true;
     }
-  });
+  };
+  size_t t = std::thread::hardware_concurrency();
+  t = std::max<size_t>(1, std::min<size_t>({t, 16, blocks}));
+  std::vector<std::thread> pool;
+  pool.reserve(t - 1);
+  for (size_t k = 1; k < t; ++k) pool.emplace_back(work, true);
+  for (size_t k = check; k < n; k += kBlock) {
+    const size_t k1 = std::min(n, k + kBlock);
+    recur(k, k1);
+    produced.store(k1, std::memory_order_release);
+  }
+  work(false);
+  for (std::thread& th : pool) th.join();
+  return !failed;
 }
 
 bool verbose() {
@@ -533,8 +574,21 @@ FFT_CFFI_API int fft_griffin_lim(void* ctx_forward, void* ctx_inverse, const flo
     // Their cosines and sines (std::cos / std::sin of the float angle, as
     // there) are evaluated by several host threads; the device multiplies
     // them by the magnitudes.
-    std::vector<float2> cs(total_bins);
-    gl_initial_phasors(seed ? seed : 0x47d7bfad, total_bins, cs.data());
+    // Both contexts are this call's for its duration (the forward one holds
+    // the working set), taken together so that no two calls deadlock.
+    std::scoped_lock lk(fc->mu, ic->mu);
+    if (fc->h_gl_cs_cap < total_bins) {
+      if (fc->h_gl_cs) cudaFreeHost(fc->h_gl_cs);
+      fc->h_gl_cs = nullptr;
+      fc->h_gl_cs_cap = 0;
+      void* hp_cs = nullptr;
+      if (cudaHostAlloc(&hp_cs, total_bins * sizeof(float2), cudaHostAllocPortable) != cudaSuccess) return 0;
+      fc->h_gl_cs = static_cast<float2*>(hp_cs);
+      fc->h_gl_cs_cap = total_bins;
+    }
+    float2* cs = fc->h_gl_cs;
+    using clk = std::chrono::steady_clock;
+    const clk::time_point t_start = clk::now();
     // The iterations run on the device (phase_infer.hpp:140-208): the inverse
     // batch, the count-normalised overlap-add, and the forward STFT whose
     // epilogue projects its spectra onto the target magnitudes, all enqueued
@@ -549,17 +603,16 @@ FFT_CFFI_API int fft_griffin_lim(void* ctx_forward, void* ctx_inverse, const flo
         if (dev >= 0) cudaSetDevice(dev);
       }
     } restore{prev != fc->device ? prev : -1};
-    DevBuf d_spec, d_frames, d_ola, d_tmp;
     const size_t fb = total_bins * sizeof(float);
-    float* mag = static_cast<float*>(d_spec.get(3 * fb));
+    float* mag = static_cast<float*>(fc->d_gl_spec.get(3 * fb));
     float* re = mag + total_bins;
     float* im = re + total_bins;
     // forward outputs of the unfused projection; first the cosines and sines
-    float* tr = static_cast<float*>(d_tmp.get(3 * fb));
+    float* tr = static_cast<float*>(fc->d_gl_tmp.get(3 * fb));
     float* ti = tr + total_bins;
     float* tm = ti + total_bins;
-    float* frame_pcm = static_cast<float*>(d_frames.get(frames * plan_n * sizeof(float)));
-    float* ola = static_cast<float*>(d_ola.get(ola_len * sizeof(float)));
+    float* frame_pcm = static_cast<float*>(fc->d_gl_frames.get(frames * plan_n * sizeof(float)));
+    float* ola = static_cast<float*>(fc->d_gl_ola.get(ola_len * sizeof(float)));
     cudaStream_t st = fc->stream;
     cudaStream_t ist = ic->stream;
     auto ok = [](cudaError_t e) {
@@ -578,9 +631,13 @@ FFT_CFFI_API int fft_griffin_lim(void* ctx_forward, void* ctx_inverse, const flo
       ok(cudaEventCreateWithFlags(&ev.fwd, cudaEventDisableTiming));
     }
     ok(cudaMemcpyAsync(mag, in_mag, fb, cudaMemcpyDefault, st));
-    ok(cudaMemcpyAsync(tr, cs.data(), 2 * fb, cudaMemcpyHostToDevice, st));
+    if (!gl_initial_phasors(seed ? seed : 0x47d7bfad, total_bins, fc->h_gl_state, cs,
+                            reinterpret_cast<float2*>(tr), fc->device, st))
+      throw std::runtime_error("cuda");
+    const clk::time_point t_phasors = clk::now();
     ok(launch_gl_init(mag, reinterpret_cast<const float2*>(tr), re, im, (long long)total_bins, st));
     ok(cudaStreamSynchronize(st));
+    const clk::time_point t_upload = clk::now();
     // The reference refines out_real/out_imag in place, so a failed pass
     // leaves the spectra of the last completed one there.
     auto flush = [&]() {
@@ -622,7 +679,18 @@ FFT_CFFI_API int fft_griffin_lim(void* ctx_forward, void* ctx_inverse, const flo
         return 0;
       }
     }
+    const clk::time_point t_enqueued = clk::now();
     flush();
+    if (verbose()) {
+      auto ms = [](clk::time_point a, clk::time_point b) {
+        return std::chrono::duration<double, std::milli>(b - a).count();
+      };
+      std::fprintf(stderr,
+                   "[diag] fft_griffin_lim: %zu bins x %d iterations: phasors %.3f ms, upload %.3f ms, "
+                   "enqueue %.3f ms, drain + copy-out %.3f ms\n",
+                   total_bins, iters, ms(t_start, t_phasors), ms(t_phasors, t_upload), ms(t_upload, t_enqueued),
+                   ms(t_enqueued, clk::now()));
+    }
     return 1;
   } catch (...) {
     return 0;

@@ -404,3 +404,40 @@ def test_config2_full_batch_seed1(kernel, inverse):
     e_out = (y.double() ** 2).sum(dim=(1, 2))
     scale = float(N) if not inverse else 1.0 / N
     assert float(((e_out / (scale * e_in)) - 1).abs().max()) < 1e-4
+
+
+@pytest.mark.parametrize("N,H", [(64, 16), (64, 24), (256, 64), (32, 32), (64, 10), (128, 12)])
+@pytest.mark.parametrize("cola", [0, 1])
+def test_overlap_add_is_the_frame_order_sum(N, H, cola):
+    # fft_cffi.cpp:1295-1320: the internal overlap-add is the float sum of the
+    # frames in frame order over frames*N samples, divided by the frame count
+    # covering each sample under COLA normalisation.  The GPU's own frames
+    # (apply_ola off) summed that way in numpy must equal its OLA output bit
+    # for bit, on the 16-byte path (N, H multiples of 4) and the scalar one.
+    nf = 37
+    bins = N // 2 + 1
+    rng = np.random.default_rng(N * 100 + H + cola)
+    re = rng.standard_normal(nf * bins).astype(np.float32)
+    im = rng.standard_normal(nf * bins).astype(np.float32)
+    base = dict(inverse=1, transform=2, half_spectrum=1, window=N, hop=H, cola_mode=cola)
+    fctx = ff.FftContext.full_v2(**ctx_kwargs(N, **base))
+    octx = ff.FftContext.full_v2(**ctx_kwargs(N, apply_ola=1, **base))
+    frames = np.zeros(nf * N, np.float32)
+    out = np.zeros(nf * N, np.float32)
+    assert fctx.execute_complex_batched(re, im, nf, frames) == nf
+    assert octx.execute_complex_batched(re, im, nf, out) == nf
+    exp = np.zeros(nf * N, np.float32)
+    cnt = np.zeros(nf * N, np.float32)
+    fr = frames.reshape(nf, N)
+    for f in range(nf):
+        s = f * H
+        e = min(s + N, nf * N)
+        if e > s:
+            exp[s:e] += fr[f, :e - s]
+            cnt[s:e] += np.float32(1)
+    if cola:
+        nz = cnt > np.float32(1e-12)
+        exp[nz] = exp[nz] / cnt[nz]
+    assert np.array_equal(out, exp)
+    fctx.close()
+    octx.close()
