@@ -662,8 +662,9 @@ def measure_griffin_lim(ff, torch, reps: int = 5):
 def measure_precision(ff, torch, stream, timed):
     """C2C N=65536 (256 x 256 four-step) x 2048, re/im N(0,1) from seed 3:
     the FP32 CUDA-core path against the split-FP16 tensor-core radix-16
-    variant (FFTFREE_TC16=1), each with its rel-L2 against an FP64 DFT of 8
-    transforms."""
+    variant (FFTFREE_TC16=1, mma.sync), each with its rel-L2 against an FP64
+    DFT of 8 transforms; and C2C N=256 x 262,144 against the tcgen05 form
+    (FFTFREE_TC16=2: tensor-memory accumulators), rel-L2 over 64 transforms."""
     import numpy as np
 
     N, B = 65536, 2048
@@ -688,6 +689,31 @@ def measure_precision(ff, torch, stream, timed):
     os.environ.pop("FFTFREE_TC16", None)
     out["kept"] = "split_fp16_tensor_core" if out["split_fp16_tensor_core"]["ms"] < out["fp32_cuda_core"]["ms"] \
         else "fp32_cuda_core"
+    del x, y
+    # 256-point transforms (one pass) x 262,144: the FP32 engine against the
+    # tcgen05 split-FP16 kernel (FFTFREE_TC16=2, k_tc05.cu)
+    N2, B2 = 256, 262144
+    z2 = rng.standard_normal((B2, N2, 2)).astype(np.float32)
+    x2 = torch.from_numpy(z2).cuda()
+    y2 = torch.empty_like(x2)
+    ref2 = np.fft.fft(z2[:64, :, 0].astype(np.float64) + 1j * z2[:64, :, 1].astype(np.float64), axis=1)
+    n256 = {}
+    for name, tc in (("fp32_cuda_core", "0"), ("split_fp16_tcgen05", "2")):
+        os.environ["FFTFREE_TC16"] = tc
+        c = ff.FftContext.full_v2(N2, kernel=2)
+        c.set_stream(stream.cuda_stream)
+        c.set_async(True)
+        r = timed(lambda: c.execute_c2c(x2, y2, B2), 16 * N2 * B2)
+        torch.cuda.synchronize()
+        got = y2[:64].cpu().numpy()
+        got = got[..., 0].astype(np.float64) + 1j * got[..., 1].astype(np.float64)
+        r["rel_l2_vs_fp64"] = float(f"{np.linalg.norm(got - ref2) / np.linalg.norm(ref2):.3e}")
+        n256[name] = r
+        c.close()
+    os.environ.pop("FFTFREE_TC16", None)
+    n256["kept"] = "split_fp16_tcgen05" if n256["split_fp16_tcgen05"]["ms"] < n256["fp32_cuda_core"]["ms"] \
+        else "fp32_cuda_core"
+    out["c2c_n256_b262144"] = n256
     return out
 
 

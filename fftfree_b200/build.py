@@ -20,7 +20,7 @@ LIB = os.path.join(HERE, "lib", "libfft_cffi.so")
 CUDA_HOME = os.environ.get("CUDA_HOME", "/usr/local/cuda")
 NVCC = os.path.join(CUDA_HOME, "bin", "nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
-CU_SOURCES = ["k_common.cu", "k_stft.cu", "k_c2c.cu", "k_cplx.cu", "k_fourstep.cu", "k_grad.cu", "k_ragged.cu", "k_2d.cu", "ft_tools.cu", "meta.cu", "noalloc.cu"]
+CU_SOURCES = ["k_common.cu", "k_stft.cu", "k_c2c.cu", "k_cplx.cu", "k_fourstep.cu", "k_grad.cu", "k_ragged.cu", "k_2d.cu", "ft_tools.cu", "meta.cu", "noalloc.cu", "k_tc05.cu"]
 CPP_SOURCES = ["abi.cpp", "recovery.cpp", "stream.cpp", "ragged.cpp"]
 
 

@@ -150,6 +150,13 @@ cudaError_t launch_cplx_batch(const CplxBatchArgs& a, int logr, cudaStream_t s, 
 cudaError_t launch_ola(const OlaArgs& a, cudaStream_t s, uint64_t* launches);
 // Griffin-Lim projection: re + i im = mag e^{i atan2(ti, tr)} (half spectrum:
 // DC and, for even N, Nyquist imaginary parts cleared).
+// 256-point C2C transforms (no hooks) on the tcgen05 tensor cores in split
+// FP16 (k_tc05.cu), chosen when FFTFREE_TC16=2; the count of blocks whose
+// bounded wait on an MMA commit gave up (their outputs are left unwritten).
+bool tc05_requested();
+cudaError_t launch_c2c256_tc05(const C2cArgs& a, cudaStream_t s, uint64_t* launches);
+unsigned tc05_timeouts();
+
 // Griffin-Lim initial spectra: re = mag * cs.x, im = mag * cs.y (cs: the
 // cosines and sines of the initial phases).
 cudaError_t launch_gl_init(const float* mag, const float2* cs, float* re, float* im, long long n, cudaStream_t s);
