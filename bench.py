@@ -202,6 +202,7 @@ CASES = {
     "r2c_n4096_polar_b8192": "R2C N=W=H=4096, half spectrum, store_polar, 8192 frames (fft_execute_batched)",
     "c2r_n4096_polar_b8192": "C2R N=4096 half spectrum polar input (Cooley-Tukey pre-hook), 8192 frames "
                              "(fft_execute_complex_batched)",
+    "c2c_n256_b262144": "C2C N=256 x 262144 complex64, one pass (FFTFREE_TC16=2: the tcgen05 split-FP16 kernel)",
     "griffin_lim_n1024_h256": "fft_griffin_lim, N=W=1024 H=256 Hann, 4096 frames x 513 bins, 32 iterations "
                               "(device magnitudes and outputs)",
 }
@@ -223,6 +224,13 @@ def run_case(args):
         c.set_stream(stream.cuda_stream)
         c.set_async(True)
         fn, nbytes = (lambda: c.execute_c2c(x, y, 8192)), 2 * x.numel() * 4
+    elif name == "c2c_n256_b262144":
+        x = torch.randn(262144, 256, 2, device="cuda", generator=g)
+        y = torch.empty_like(x)
+        c = ff.FftContext.full_v2(256, kernel=2)
+        c.set_stream(stream.cuda_stream)
+        c.set_async(True)
+        fn, nbytes = (lambda: c.execute_c2c(x, y, 262144)), 2 * x.numel() * 4
     elif name == "c2c_n65536_b512":
         x = torch.randn(512, 65536, 2, device="cuda", generator=g)
         y = torch.empty_like(x)

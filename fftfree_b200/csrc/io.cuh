@@ -42,7 +42,9 @@ __device__ __forceinline__ float atan2_fast(float y, float x) {
     mx *= sc;
     mn *= sc;
   }
-  const float a = __fdividef(mn, mx);
+  // both zero: a = 0, which the octant steps below turn into C's atan2 of
+  // signed zeros (0, or pi for x = -0, with the sign of y)
+  const float a = (mx > 0.f) ? __fdividef(mn, mx) : 0.f;
   const float t = a * a;
   float p = -0.004780322778970003f;
   p = fmaf(p, t, 0.024556664749979973f);
@@ -55,7 +57,6 @@ __device__ __forceinline__ float atan2_fast(float y, float x) {
   float r = a * p;
   if (ay > ax) r = 1.5707963705062866f - r;
   if (signbit(x)) r = 3.1415927410125732f - r;
-  if (ax == 0.f && ay == 0.f) r = signbit(x) ? 3.1415927410125732f : 0.f;
   return copysignf(r, y);
 }
 
