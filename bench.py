@@ -65,18 +65,53 @@ def _profile_traffic():
 
 
 class ClockSampler:
-    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+    """SM clocks, power and throttle reasons sampled during the timed region:
+    through NVML (opened before the region, one sample as it starts, then
+    every millisecond, one as it ends: the region may last only
+    milliseconds), nvidia-smi every 200 ms where NVML is unavailable.
+    Reads only."""
 
     def __init__(self, index: int):
         self.index = index
         self.samples = []
+        self.source = None
         self._stop = threading.Event()
         self._t = None
+        self._nvml = None
+
+    def _open_nvml(self):
+        import pynvml
+        pynvml.nvmlInit()
+        h = pynvml.nvmlDeviceGetHandleByIndex(self.index)
+        bits = [getattr(pynvml, "nvmlClocksEventReasonHwSlowdown", 0x8),
+                getattr(pynvml, "nvmlClocksEventReasonHwThermalSlowdown", 0x40),
+                getattr(pynvml, "nvmlClocksEventReasonSwThermalSlowdown", 0x20),
+                getattr(pynvml, "nvmlClocksEventReasonSwPowerCap", 0x4)]
+        reasons = getattr(pynvml, "nvmlDeviceGetCurrentClocksEventReasons", None) or \
+            pynvml.nvmlDeviceGetCurrentClocksThrottleReasons
+        mx = pynvml.nvmlDeviceGetMaxClockInfo(h, pynvml.NVML_CLOCK_SM)
+        self._nvml = (pynvml, h, bits, reasons, mx)
+        self.source = "nvml, 1 ms"
+
+    def _sample_nvml(self):
+        pynvml, h, bits, reasons, mx = self._nvml
+        sm = pynvml.nvmlDeviceGetClockInfo(h, pynvml.NVML_CLOCK_SM)
+        pw = pynvml.nvmlDeviceGetPowerUsage(h) / 1000.0
+        r = reasons(h)
+        self.samples.append([str(sm), str(mx), f"{pw:.1f}"] + ["Active" if r & b else "Not Active" for b in bits])
 
     def _run(self):
+        if self._nvml:
+            try:
+                while not self._stop.wait(0.001):
+                    self._sample_nvml()
+                return
+            except Exception:
+                pass
         q = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
              "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
              "clocks_event_reasons.sw_power_cap")
+        self.source = "nvidia-smi, 200 ms"
         while not self._stop.is_set():
             try:
                 out = subprocess.run(["nvidia-smi", "-i", str(self.index), f"--query-gpu={q}",
@@ -89,6 +124,11 @@ class ClockSampler:
             self._stop.wait(0.2)
 
     def __enter__(self):
+        try:
+            self._open_nvml()
+            self._sample_nvml()
+        except Exception:
+            self._nvml = None
         self._t = threading.Thread(target=self._run, daemon=True)
         self._t.start()
         return self
@@ -97,6 +137,12 @@ class ClockSampler:
         self._stop.set()
         if self._t:
             self._t.join(timeout=10)
+        if self._nvml:
+            try:
+                self._sample_nvml()
+                self._nvml[0].nvmlShutdown()
+            except Exception:
+                pass
 
     def summary(self):
         if not self.samples:
@@ -107,7 +153,7 @@ class ClockSampler:
         reasons = sorted({names[i] for s in self.samples for i in range(4) if len(s) > 3 + i and
                           s[3 + i].lower().startswith("active")})
         return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
-                "reasons": reasons, "samples": len(self.samples)}
+                "reasons": reasons, "samples": len(self.samples), "source": self.source}
 
 
 def _seed1_batch(seed: int = 1):

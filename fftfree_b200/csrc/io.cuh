@@ -7,6 +7,8 @@
 
 #include <stdint.h>
 
+#include <type_traits>
+
 #include "fft_engine.cuh"
 #include "kernels.h"
 
@@ -432,32 +434,47 @@ struct StftIO {
         }
         return;
       }
+      // store_polar's magnitude array: |X| itself when it mirrors the real
+      // output (fft_execute_batched), else |(|X|, arg X)| -- a uniform
+      // choice, taken once outside the unrolled loop
+      const auto bins_loop = [&](auto mag_re) {
 #pragma unroll
-      for (int i = 0; i < R; ++i) {
-        const float2 zm = sm[pidx((M - t - i * T) & (M - 1))];
-        float2 X = untangle_bin(v[i], zm, w.half(i));
-        if (i == 0 && t == 0) X.y = 0.f;  // DC
-        if constexpr (MODE == 4) {
-          float m;
-          reinterpret_cast<float2*>(re)[t + i * T] = mag_phasor(X, &m);
-          pm[i * T] = m;
-          continue;
+        for (int i = 0; i < R; ++i) {
+          const float2 zm = sm[pidx((M - t - i * T) & (M - 1))];
+          float2 X = untangle_bin(v[i], zm, w.half(i));
+          if (i == 0 && t == 0) X.y = 0.f;  // DC
+          if constexpr (MODE == 4) {
+            float m;
+            reinterpret_cast<float2*>(re)[t + i * T] = mag_phasor(X, &m);
+            pm[i * T] = m;
+            continue;
+          }
+          if constexpr (MODE == 3) {
+            pm[i * T] = cabs_fast(X.x, X.y);
+            continue;
+          }
+          float mag;
+          if constexpr (MODE == 2) {
+            mag = cabs_fast(X.x, X.y);
+            X = make_float2(mag, atan2_fast(X.y, X.x));
+            if constexpr (!decltype(mag_re)::value) mag = cabs_fast(X.x, X.y);
+          } else if constexpr (MODE == 1) {
+            mag = cabs_fast(X.x, X.y);
+            X = make_float2(mag, 0.f);
+          } else {
+            if (a.pf.clear_imag) X.y = 0.f;
+            mag = cabs_fast(X.x, X.y);
+          }
+          pr[i * T] = X.x;
+          pi[i * T] = X.y;
+          pm[i * T] = mag;
         }
-        if constexpr (MODE == 3) {
-          pm[i * T] = cabs_fast(X.x, X.y);
-          continue;
-        }
-        float mag;
-        if constexpr (MODE == 2) { mag = cabs_fast(X.x, X.y); X = make_float2(mag, atan2_fast(X.y, X.x)); }
-        else if constexpr (MODE == 1) { mag = cabs_fast(X.x, X.y); X = make_float2(mag, 0.f); }
-        else {
-          if (a.pf.clear_imag) X.y = 0.f;
-          mag = cabs_fast(X.x, X.y);
-        }
-        if constexpr (MODE == 2) mag = a.mag_from_real ? X.x : cabs_fast(X.x, X.y);
-        pr[i * T] = X.x;
-        pi[i * T] = X.y;
-        pm[i * T] = mag;
+      };
+      if constexpr (MODE == 2) {
+        if (a.mag_from_real) bins_loop(std::true_type{});
+        else bins_loop(std::false_type{});
+      } else {
+        bins_loop(std::true_type{});
       }
       if (t == 0) emit(re, im, mg, M, make_float2(v[0].x - v[0].y, 0.f), true, inv_n, mag_is_re);
       return;
