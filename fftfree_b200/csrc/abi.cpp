@@ -1282,7 +1282,9 @@ static int mag_grad_run() {
     const char* e = std::getenv("FFTFREE_GRAD_RUN");
     return e ? std::atoi(e) : -1;
   }();
-  return env >= 0 ? env : 32;  // frames per thread group; 0 selects the general form
+  // frames per thread group (FFTFREE_GRAD_RUN, for sweeps); 0 selects the
+  // general form, -1 lets the launcher fit the runs to the GPU
+  return env >= 0 ? env : -1;
 }
 
 // Shared body of the magnitude STFT entry points; out_phasor (X / |X| as

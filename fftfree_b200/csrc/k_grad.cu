@@ -123,8 +123,10 @@ constexpr int grad_min_blocks() {
 // Hermitian half spectrum y (bins t + i*T, the Nyquist bin in ynyq on
 // thread 0; DC and Nyquist already doubled) to the windowed frame gradient:
 // v[i] holds samples n = 2m, 2m+1 (m = t + i*T) of w[n] dL/ds[n], zero from
-// `cnt` on.  The tile must be free on entry; it is free on return.
-template <class S>
+// `cnt` on.  RAW leaves the window and the count to the caller: v[i] =
+// (dL/ds[2m], -dL/ds[2m+1]).  The tile must be free on entry; it is free on
+// return.
+template <class S, bool RAW = false>
 __device__ __forceinline__ void grad_inverse(const MagGradArgs& a, const float2 (&y)[S::R], float2 ynyq,
                                              long long cnt, int t, float2* sm, const Twiddles& tw,
                                              float2 (&v)[S::R]) {
@@ -153,6 +155,7 @@ __device__ __forceinline__ void grad_inverse(const MagGradArgs& a, const float2 
   }
   GroupSync::sync<S>();  // the engine reuses the tile
   fft_engine<S, GroupSync>(v, t, sm, tw);
+  if constexpr (RAW) return;
 
   // dL/ds[2m] = Re, dL/ds[2m+1] = -Im, times the window, zero past the frame's samples.
 #pragma unroll
@@ -173,7 +176,7 @@ __device__ __forceinline__ void grad_inverse(const MagGradArgs& a, const float2 
 // n = 2m, 2m + 1 (m = t + i*T) of w[n] dL/ds_f[n], zero from the frame's
 // sample count on.  Every group barrier is inside; the tile is free on
 // return (its last reads are behind a barrier).
-template <class S>
+template <class S, bool RAW = false>
 __device__ __forceinline__ void frame_grad(const MagGradArgs& a, const float* pcm, const float* gsig, long long f,
                                            bool ok, int t, float2* sm, const Twiddles& tw, float2 (&v)[S::R]) {
   constexpr int T = S::T, R = S::R, M = S::M;
@@ -214,12 +217,12 @@ __device__ __forceinline__ void frame_grad(const MagGradArgs& a, const float* pc
     ynyq = make_float2(2.f * mag_chain(make_float2(xn, 0.f), gn).x, 0.f);
   }
   GroupSync::sync<S>();  // every read of Z is done
-  grad_inverse<S>(a, y, ynyq, cnt, t, sm, tw, v);
+  grad_inverse<S, RAW>(a, y, ynyq, cnt, t, sm, tw, v);
 }
 
 // The same from the unit phasor U = X / |X| the forward pass saved:
 // V = g U -- no forward transform, no signal read.
-template <class S>
+template <class S, bool RAW = false>
 __device__ __forceinline__ void frame_grad_phasor(const MagGradArgs& a, const float* gsig, const float2* usig,
                                                   long long f, bool ok, int t, float2* sm, const Twiddles& tw,
                                                   float2 (&v)[S::R]) {
@@ -241,15 +244,15 @@ __device__ __forceinline__ void frame_grad_phasor(const MagGradArgs& a, const fl
   }
   float2 ynyq = make_float2(0.f, 0.f);
   if (t == 0 && ok) ynyq = make_float2(2.f * sc * __ldg(gsig + off + M) * __ldg(usig + off + M).x, 0.f);  // Nyquist
-  grad_inverse<S>(a, y, ynyq, cnt, t, sm, tw, v);
+  grad_inverse<S, RAW>(a, y, ynyq, cnt, t, sm, tw, v);
 }
 
-template <class S, bool PH>
+template <class S, bool PH, bool RAW = false>
 __device__ __forceinline__ void frame_grad_any(const MagGradArgs& a, const float* pcm, const float2* psig,
                                                const float* gsig, long long f, bool ok, int t, float2* sm,
                                                const Twiddles& tw, float2 (&v)[S::R]) {
-  if constexpr (PH) frame_grad_phasor<S>(a, gsig, psig, f, ok, t, sm, tw, v);
-  else frame_grad<S>(a, pcm, gsig, f, ok, t, sm, tw, v);
+  if constexpr (PH) frame_grad_phasor<S, RAW>(a, gsig, psig, f, ok, t, sm, tw, v);
+  else frame_grad<S, RAW>(a, pcm, gsig, f, ok, t, sm, tw, v);
 }
 
 // General form: each block owns `span` samples of one signal and gathers
@@ -334,6 +337,69 @@ constexpr int slide_min_blocks() {
   return want < fit80 ? want : (fit80 > 1 ? fit80 : 1);
 }
 
+// Two samples p, p + 1 of the output (p even), as one 8-byte store where
+// the row is 8-byte aligned and both are inside the signal.
+__device__ __forceinline__ void store_pair(float* out, long long p, long long L, float x0, float x1, bool vec) {
+  if (vec && p + 1 < L) {
+    *reinterpret_cast<float2*>(out + p) = make_float2(x0, x1);
+  } else {
+    if (p < L) out[p] = x0;
+    if (p + 1 < L) out[p + 1] = x1;
+  }
+}
+
+// One frame into the register window at rotation ROT: slot i of the frame
+// (samples 2(t + iT) + {0, 1} past its start) adds into acc[(i + ROT*SH) % R]
+// as one FFMA2 with the window taps; v holds (dL/ds[2m], -dL/ds[2m+1]), so
+// the window keeps the second sum negated.  The SH slots that are then
+// complete (acc[ROT*SH ..]) are written when `store` and cleared for the
+// frames to come.  Rotating the window instead of shifting it costs no
+// register moves.
+template <class S, int QL, int ROT>
+__device__ __forceinline__ void slide_step(float2 (&acc)[S::R], const float2 (&v)[S::R], const float2* w2, int t,
+                                           bool store, float* out, long long base, long long L, bool vec) {
+  constexpr int T = S::T, R = S::R, SH = R >> QL;
+#pragma unroll
+  for (int i = 0; i < R; ++i) {
+    const float2 w = w2 ? __ldg(w2 + t + i * T) : make_float2(1.f, 1.f);
+    acc[(i + ROT * SH) % R] = __ffma2_rn(v[i], w, acc[(i + ROT * SH) % R]);
+  }
+  if (store) {
+#pragma unroll
+    for (int j = 0; j < SH; ++j)
+      store_pair(out, base + 2 * (t + j * T), L, acc[ROT * SH + j].x, -acc[ROT * SH + j].y, vec);
+  }
+#pragma unroll
+  for (int j = 0; j < SH; ++j) acc[ROT * SH + j] = make_float2(0.f, 0.f);
+}
+
+template <class S, int QL, int ROT = 0>
+__device__ __forceinline__ void slide_step_at(int rot, float2 (&acc)[S::R], const float2 (&v)[S::R],
+                                              const float2* w2, int t, bool store, float* out, long long base,
+                                              long long L, bool vec) {
+  if constexpr (ROT < (1 << QL)) {
+    if (rot == ROT) slide_step<S, QL, ROT>(acc, v, w2, t, store, out, base, L, vec);
+    else slide_step_at<S, QL, ROT + 1>(rot, acc, v, w2, t, store, out, base, L, vec);
+  }
+}
+
+// After the last frame: the slots still pending (relative slots 0 .. R-SH-1
+// of the frame that would follow, at rotation ROT) go out.
+template <class S, int QL, int ROT = 0>
+__device__ __forceinline__ void slide_tail_at(int rot, const float2 (&acc)[S::R], int t, float* out, long long base,
+                                              long long L, bool vec) {
+  constexpr int T = S::T, R = S::R, SH = R >> QL;
+  if constexpr (ROT < (1 << QL)) {
+    if (rot == ROT) {
+#pragma unroll
+      for (int i = 0; i < R - SH; ++i)
+        store_pair(out, base + 2 * (t + i * T), L, acc[(ROT * SH + i) % R].x, -acc[(ROT * SH + i) % R].y, vec);
+    } else {
+      slide_tail_at<S, QL, ROT + 1>(rot, acc, t, out, base, L, vec);
+    }
+  }
+}
+
 template <class S, int QL, bool PH>
 __global__ void __launch_bounds__(Launch<S>::BLOCK, slide_min_blocks<S>()) k_stft_mag_grad_slide(MagGradArgs a,
                                                                                                  Twiddles tw) {
@@ -357,37 +423,34 @@ __global__ void __launch_bounds__(Launch<S>::BLOCK, slide_min_blocks<S>()) k_stf
   const float2* psig = PH ? a.phasor + sig * a.frames * (long long)(M + 1) : nullptr;
   float* out = a.grad_pcm + sig * a.sig_stride;
   const long long L = a.pcm_len;
+  const bool vec = aligned8(out);
+  const float2* w2 = reinterpret_cast<const float2*>(a.win);  // 8-byte aligned (checked by the launcher)
 
   float2 acc[R];
 #pragma unroll
   for (int i = 0; i < R; ++i) acc[i] = make_float2(0.f, 0.f);
+  int rot = 0;
   for (long long f = f_start; f < f_end; ++f) {
     float2 v[R];
-    frame_grad_any<S, PH>(a, pcm, psig, gsig, f, true, t, sm, tw, v);
+    frame_grad_any<S, PH, true>(a, pcm, psig, gsig, f, true, t, sm, tw, v);
+    long long cnt = L - f * (long long)a.H;  // the frame's samples; zero padding from there on
+    if (cnt > a.W) cnt = a.W;
+    if (cnt < 2 * M) {
 #pragma unroll
-    for (int i = 0; i < R; ++i) acc[i] = cadd(acc[i], v[i]);
-    if (f >= f_own) {  // samples f*H .. f*H + H - 1 are complete
-      const long long base = f * (long long)a.H;
-#pragma unroll
-      for (int i = 0; i < SH; ++i) {
-        const long long p = base + 2 * (t + i * T);
-        if (p < L) out[p] = acc[i].x;
-        if (p + 1 < L) out[p + 1] = acc[i].y;
+      for (int i = 0; i < R; ++i) {
+        const int n = 2 * (t + i * T);
+        if (n >= cnt) v[i].x = 0.f;
+        if (n + 1 >= cnt) v[i].y = 0.f;
       }
     }
-#pragma unroll
-    for (int i = 0; i < R; ++i) acc[i] = (i + SH < R) ? acc[i + SH] : make_float2(0.f, 0.f);
+    slide_step_at<S, QL>(rot, acc, v, w2, t, f >= f_own, out, f * (long long)a.H, L, vec);
+    rot = (rot + 1) & ((1 << QL) - 1);
   }
   if (f_end == a.frames) {
     // the last run also writes the tail of the last frame and zeros the
     // samples no frame covers
     const long long base = f_end * (long long)a.H;
-#pragma unroll
-    for (int i = 0; i < R - SH; ++i) {
-      const long long p = base + 2 * (t + i * T);
-      if (p < L) out[p] = acc[i].x;
-      if (p + 1 < L) out[p + 1] = acc[i].y;
-    }
+    slide_tail_at<S, QL>(rot, acc, t, out, base, L, vec);
     for (long long p = base + 2LL * (R - SH) * T + t; p < L; p += T) out[p] = 0.f;
   }
 }
@@ -406,8 +469,35 @@ static int slide_logr(int logm) {
   return (logm == 10) ? 4 : 3;
 }
 
+// Frames per thread group when the caller leaves it open (run < 0): among
+// runs of 16 .. 64 frames, the one with the least work per group slot, a
+// group slot being one of the G groups of a block resident on an SM.  Each
+// group also transforms the `halo` frames before its run, and all groups take
+// equally long, so a launch costs about ceil(jobs / slots) * (run + halo)
+// frame transforms per slot.  On 64 signals of 509 frames (H = N/4, 1184
+// slots) that is a run of 29: 1152 groups in one wave, where runs of 32 would
+// leave 40 SMs with one block instead of two.
+static long long slide_run(const MagGradArgs& a, const void* fn, int block, size_t smem, int G, int halo) {
+  if (a.run > 0) return a.run;
+  int dev = 0, sms = 0, per_sm = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) !=
+      cudaSuccess || cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, block, smem) != cudaSuccess ||
+      per_sm < 1) {
+    cudaGetLastError();
+    return 32;
+  }
+  const long long slots = (long long)sms * per_sm * G;
+  long long best = 32, best_cost = -1;
+  for (long long run = 16; run <= 64; ++run) {
+    const long long jobs = a.signals * ((a.frames + run - 1) / run);
+    const long long cost = ((jobs + slots - 1) / slots) * (run + halo);
+    if (best_cost < 0 || cost < best_cost) best = run, best_cost = cost;
+  }
+  return best;
+}
+
 template <class S, int QL, bool PH>
-static cudaError_t launch_slide(const MagGradArgs& a, cudaStream_t st, uint64_t* launches) {
+static cudaError_t launch_slide(const MagGradArgs& a0, cudaStream_t st, uint64_t* launches) {
   using L = Launch<S>;
   const size_t smem = (size_t)L::G * S::SMEM * sizeof(float2);
   if (smem > 48 * 1024) {
@@ -415,6 +505,8 @@ static cudaError_t launch_slide(const MagGradArgs& a, cudaStream_t st, uint64_t*
                                                cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
   }
+  MagGradArgs a = a0;
+  a.run = (int)slide_run(a0, (const void*)k_stft_mag_grad_slide<S, QL, PH>, L::BLOCK, smem, L::G, (1 << QL) - 1);
   const long long jobs = a.signals * ((a.frames + a.run - 1) / a.run);
   const long long grid = (jobs + L::G - 1) / L::G;
   if (grid > 0x7fffffffLL) return cudaErrorInvalidValue;
@@ -431,8 +523,9 @@ cudaError_t launch_stft_mag_grad(const MagGradArgs& a, int req_logr, cudaStream_
   const int logm = ilog2i(a.N) - 1;
   if (logm + 1 > max_mag_grad_log()) return cudaErrorInvalidValue;
 
-  // Sliding form when the hop is N / 2^q (q <= 3) and a multiple of 2T.
-  if (a.run > 0 && logm >= 6 && (a.N % a.H) == 0) {
+  // Sliding form when the hop is N / 2^q (q <= 3) and a multiple of 2T
+  // (and the window taps can be read in pairs).
+  if (a.run != 0 && logm >= 6 && (a.N % a.H) == 0 && (reinterpret_cast<uintptr_t>(a.win) & 7) == 0) {
     const int q = ilog2i(a.N / a.H);
     const int lr = slide_logr(logm);
     const int T = 1 << (logm - lr);

@@ -67,7 +67,8 @@ struct MagGradArgs {
   const float2* phasor;   // saved X / |X|, same layout (0 at |X| = 0); nullptr: recompute from pcm
   float* grad_pcm;        // signals x sig_stride; every sample < pcm_len written
   int span;               // general form: samples of one signal owned by one block
-  int run;                // sliding form: frames of one signal per thread group (0: general form only)
+  int run;                // sliding form: frames of one signal per thread group (0: general form only,
+                          // < 0: chosen by the launcher)
   // the gradient is scaled by factor (times *scale when not null, a device
   // scalar: the upstream gradient of a loss, read without a host sync)
   float factor;
