@@ -155,20 +155,20 @@ __device__ __forceinline__ void grad_inverse(const MagGradArgs& a, const float2 
   }
   GroupSync::sync<S>();  // the engine reuses the tile
   fft_engine<S, GroupSync>(v, t, sm, tw);
-  if constexpr (RAW) return;
-
-  // dL/ds[2m] = Re, dL/ds[2m+1] = -Im, times the window, zero past the frame's samples.
+  if constexpr (!RAW) {
+    // dL/ds[2m] = Re, dL/ds[2m+1] = -Im, times the window, zero past the frame's samples.
 #pragma unroll
-  for (int i = 0; i < R; ++i) {
-    const int n = 2 * (t + i * T);
-    float d0 = v[i].x, d1 = -v[i].y;
-    if (a.win) {
-      d0 *= __ldg(a.win + n);
-      d1 *= __ldg(a.win + n + 1);
+    for (int i = 0; i < R; ++i) {
+      const int n = 2 * (t + i * T);
+      float d0 = v[i].x, d1 = -v[i].y;
+      if (a.win) {
+        d0 *= __ldg(a.win + n);
+        d1 *= __ldg(a.win + n + 1);
+      }
+      if (n >= cnt) d0 = 0.f;
+      if (n + 1 >= cnt) d1 = 0.f;
+      v[i] = make_float2(d0, d1);
     }
-    if (n >= cnt) d0 = 0.f;
-    if (n + 1 >= cnt) d1 = 0.f;
-    v[i] = make_float2(d0, d1);
   }
 }
 

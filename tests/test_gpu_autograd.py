@@ -68,6 +68,7 @@ CASES = [
     (2, 10000, 256, 256, 256, None),
     (2, 100, 512, 512, 128, "hann"),
     (1, 300000, 8192, 8192, 2048, "hann"),
+    (2, 26624, 2048, 2048, 512, "hann"),  # 49 frames: three runs of 16 and a last run of one frame
 ]
 
 
