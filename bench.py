@@ -206,17 +206,50 @@ def _cpu_reference_run(steps: int, warmup: int, budget_s: float = None):
     return dt, threads, kind, sample
 
 
+def _in_child(func: str, attempts: int = 3, **kw):
+    """Runs bench.<func>(**kw) in a fresh Python process (no CUDA context) and
+    returns its JSON-able result, or None when every attempt died.  The
+    reference's WorkerPool has crashed intermittently on the GPU box's 16
+    host threads (a segfault or abort in its own code, during or after a
+    call); in a child process such a crash costs one attempt, not the bench."""
+    code = ("import json, sys; sys.path.insert(0, %r); import bench; "
+            "print('@@RESULT ' + json.dumps(bench.%s(**json.loads(sys.argv[1]))), flush=True)" % (REPO, func))
+    for _ in range(attempts):
+        try:
+            r = subprocess.run([sys.executable, "-c", code, json.dumps(kw)], capture_output=True, text=True,
+                               timeout=900)
+        except subprocess.TimeoutExpired:
+            continue
+        for line in r.stdout.splitlines():
+            if line.startswith("@@RESULT "):
+                return json.loads(line[len("@@RESULT "):])
+    return None
+
+
+def _cpu_reference_child(steps: int, warmup: int, budget_s: float = None):
+    dt, threads, kind, sample = _cpu_reference_run(steps=steps, warmup=warmup, budget_s=budget_s)
+    return {"dt": dt, "threads": threads, "kind": kind, "sample": sample}
+
+
 def cpu_baseline(budget_s: float = 15.0):
-    """The reference's CPU path on the host cores (bounded: about budget_s)."""
-    dt, threads, kind, sample = _cpu_reference_run(steps=1000, warmup=1, budget_s=budget_s)
-    return {"value": round(BYTES_PER_PASS / dt / 1e9, 3), "unit": "GB/s", "cores": threads, "kind": kind,
-            "sample": sample}
+    """The reference's CPU path on the host cores (bounded: about budget_s),
+    in a child process."""
+    r = _in_child("_cpu_reference_child", steps=1000, warmup=1, budget_s=budget_s)
+    if r is None:
+        return {"unavailable": "the reference's CPU run crashed in every attempt (its WorkerPool)"}
+    return {"value": round(BYTES_PER_PASS / r["dt"] / 1e9, 3), "unit": "GB/s", "cores": r["threads"],
+            "kind": r["kind"], "sample": r["sample"]}
 
 
 def run_reference(args, rank, world):
     if rank != 0:
         return 0
-    dt, threads, kind, sample = _cpu_reference_run(steps=args.steps, warmup=args.warmup)
+    r = _in_child("_cpu_reference_child", steps=args.steps, warmup=args.warmup)
+    if r is None:
+        print(json.dumps({"impl": "reference", "unavailable": "the reference's CPU run crashed in every attempt "
+                                                              "(a segfault in its own WorkerPool)"}), flush=True)
+        return 0
+    dt, threads, kind, sample = r["dt"], r["threads"], r["kind"], r["sample"]
     value = BYTES_PER_PASS / dt / 1e9
     line = {"impl": "reference", "metric": METRIC, "value": round(value, 3), "unit": "GB/s", "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(dt * 1e3, 3),
@@ -645,8 +678,7 @@ def measure_griffin_lim(ff, torch, reps: int = 5):
     wall clock per synchronous call at 32 iterations, and the per-iteration
     cost from the 32- and 96-iteration calls.  Beside it the reference's own
     Griffin-Lim (oracle/_ref release build, host buffers, all host cores up
-    to 16) on the same shape at 2 and 4 iterations."""
-    import numpy as np
+    to 16) on the same shape at 2 and 4 iterations, in a child process."""
     N, H, F = 1024, 256, 4096
     bins = N // 2 + 1
     g = torch.Generator(device="cuda").manual_seed(5)
@@ -676,41 +708,46 @@ def measure_griffin_lim(ff, torch, reps: int = 5):
            "setup_ms": round(ms32 - 32 * (ms96 - ms32) / 64, 3)}
     fc.close()
     ic.close()
-    try:
-        from oracle import reflib
-        if os.path.exists(reflib.release_path()):
-            RL = reflib.release_lib()
-            th = max(1, min(16, os.cpu_count() or 1))
-            base = dict(n=N, threads=th, lanes=1, inverse=0, kernel=2, radix=0, radix_pattern=None, pad_mode=1,
-                        window=N, hop=H, transform=1, reduce_magnitude=0, store_polar=0, half_spectrum=1,
-                        allow_outer_parallel=1, allow_inner_parallel=0, inner_threads=0, save_crash_logs=0,
-                        silent_crash_reports=1, apply_windows=0, apply_ola=0, analysis_kind=0, analysis_p1=0.0,
-                        analysis_p2=0.0, synthesis_kind=0, synthesis_p1=0.0, synthesis_p2=0.0, norm_policy=0,
-                        cola_mode=0)
-            fk = dict(base, apply_windows=1, analysis_kind=1)
-            ik = dict(base, inverse=1, transform=2)
-            rf, ri = reflib.RefContext.full_v2(RL, **fk), reflib.RefContext.full_v2(RL, **ik)
-            hm = mag.cpu().numpy()
-            hr, hi = np.zeros_like(hm), np.zeros_like(hm)
-
-            def ref_ms(iters):
-                t0 = time.perf_counter()
-                if RL.fft_griffin_lim(rf.h, ri.h, reflib.fp(hm), F, H, 1, iters, 1, 7, reflib.fp(hr),
-                                      reflib.fp(hi)) != 1:
-                    raise RuntimeError("reference fft_griffin_lim failed")
-                return (time.perf_counter() - t0) * 1e3
-
-            r2, r4 = ref_ms(2), ref_ms(4)
-            per = (r4 - r2) / 2
-            leg["cpu_baseline"] = {"kind": "reference", "threads": th, "ms_per_iteration": round(per, 2),
-                                    "setup_ms": round(r2 - 2 * per, 2),
-                                    "ms_per_call_32_iterations_projected": round(r2 + 30 * per, 1),
-                                    "sample": "2- and 4-iteration calls, same shape and magnitudes"}
-            rf.close()
-            ri.close()
-    except Exception as e:  # the GPU figures stand without the reference beside them
-        leg["cpu_baseline"] = {"unavailable": str(e)[:200]}
+    ref = _in_child("_ref_griffin_lim", N=N, H=H, F=F)
+    leg["cpu_baseline"] = ref if ref is not None else {
+        "unavailable": "the reference's fft_griffin_lim crashed in every attempt (its WorkerPool)"}
     return leg
+
+
+def _ref_griffin_lim(N: int, H: int, F: int):
+    """The reference's own fft_griffin_lim (oracle/_ref release build, host
+    buffers, all host cores up to 16) at 2 and 4 iterations on F frames of
+    N/2 + 1 magnitudes U[0, 1) (numpy seed 5); run in a child process."""
+    import numpy as np
+    from oracle import reflib
+    if not os.path.exists(reflib.release_path()):
+        return {"unavailable": "the reference's release build is absent"}
+    RL = reflib.release_lib()
+    th = max(1, min(16, os.cpu_count() or 1))
+    base = dict(n=N, threads=th, lanes=1, inverse=0, kernel=2, radix=0, radix_pattern=None, pad_mode=1,
+                window=N, hop=H, transform=1, reduce_magnitude=0, store_polar=0, half_spectrum=1,
+                allow_outer_parallel=1, allow_inner_parallel=0, inner_threads=0, save_crash_logs=0,
+                silent_crash_reports=1, apply_windows=0, apply_ola=0, analysis_kind=0, analysis_p1=0.0,
+                analysis_p2=0.0, synthesis_kind=0, synthesis_p1=0.0, synthesis_p2=0.0, norm_policy=0,
+                cola_mode=0)
+    rf = reflib.RefContext.full_v2(RL, **dict(base, apply_windows=1, analysis_kind=1))
+    ri = reflib.RefContext.full_v2(RL, **dict(base, inverse=1, transform=2))
+    hm = np.random.default_rng(5).random(F * (N // 2 + 1)).astype(np.float32)
+    hr, hi = np.zeros_like(hm), np.zeros_like(hm)
+
+    def ref_ms(iters):
+        t0 = time.perf_counter()
+        if RL.fft_griffin_lim(rf.h, ri.h, reflib.fp(hm), F, H, 1, iters, 1, 7, reflib.fp(hr), reflib.fp(hi)) != 1:
+            raise RuntimeError("reference fft_griffin_lim failed")
+        return (time.perf_counter() - t0) * 1e3
+
+    r2, r4 = ref_ms(2), ref_ms(4)
+    per = (r4 - r2) / 2
+    rf.close()
+    ri.close()
+    return {"kind": "reference", "threads": th, "ms_per_iteration": round(per, 2), "setup_ms": round(r2 - 2 * per, 2),
+            "ms_per_call_32_iterations_projected": round(r2 + 30 * per, 1),
+            "sample": "2- and 4-iteration calls, same shape, magnitudes U[0, 1) (numpy seed 5)"}
 
 
 def measure_precision(ff, torch, stream, timed):
