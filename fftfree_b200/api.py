@@ -131,6 +131,7 @@ _SIGS = [
     ("fftfree_ragged_samples", ctypes.c_size_t, [ctypes.c_void_p]),
     ("fftfree_ragged_bins", ctypes.c_size_t, [ctypes.c_void_p]),
     ("fftfree_ragged_schedule", ctypes.c_int, [ctypes.c_void_p, ctypes.c_size_t]),
+    ("fftfree_ragged_tile", ctypes.c_int, [ctypes.c_void_p, ctypes.c_size_t]),
     ("fftfree_ragged_set_stream", None, [ctypes.c_void_p, ctypes.c_void_p]),
     ("fftfree_ragged_execute", ctypes.c_int, [ctypes.c_void_p, c_float_p, c_float_p, c_float_p, c_float_p]),
     ("fftfree_ragged_launch_count", ctypes.c_ulonglong, [ctypes.c_void_p]),
@@ -385,6 +386,9 @@ class RaggedPlan:
 
     def schedule(self, n) -> int:
         return int(lib().fftfree_ragged_schedule(self.handle, n))
+
+    def tile(self, n) -> int:
+        return int(lib().fftfree_ragged_tile(self.handle, n))
 
     def set_stream(self, stream_handle):
         lib().fftfree_ragged_set_stream(self.handle, ctypes.c_void_p(stream_handle or 0))

@@ -10,7 +10,8 @@
 // the blocks (1024 threads, one per SM) take tiles from an atomic counter
 // until the list is exhausted.  A tile is
 //  * a group of same-size frames of up to 2^14 complex points, one per
-//    T-thread slice of the block -- the single-pass engine and the STFT
+//    T-thread slice of the block, in one or more block-loads taken one after
+//    the other (the tile size the tuner picks) -- the single-pass engine and the STFT
 //    load / store policy of fft_execute_batched, so a frame matches that
 //    call bit for bit where the radix is the same; 2^14 points take the
 //    whole block (T = 1024, the transform held in registers and 139 KB of
@@ -34,33 +35,39 @@ constexpr int kFullLog = 14;   // one-block single pass
 template <class S, int MODE>
 __device__ __forceinline__ void ragged_single(const RaggedArgs& a, int4 tile, float2* smem, const Twiddles& tw) {
   constexpr int T = S::T;
+  constexpr int G = kBlock / T;  // frames the block holds at once
   static_assert(T <= 32 || kBlock / T <= 15 || T >= 256, "named barrier per group");
   const int g = threadIdx.x / T;
   const int t = threadIdx.x - g * T;
-  const bool ok = g < tile.y;
-  const int2 job = __ldg(a.jobs + tile.x + (ok ? g : 0));
-  const RaggedItem it = a.items[job.x];
-  StftArgs sa{};
-  sa.pcm = a.pcm + it.pcm_off;
-  sa.pcm_len = it.pcm_len;
-  sa.frames = ok ? (long long)job.y + 1 : 0;  // frame job.y of the item (none when !ok)
-  sa.N = 2 * S::M;
-  sa.W = it.W;
-  sa.H = it.H;
-  sa.win = it.win_off >= 0 ? a.windows + it.win_off : nullptr;
-  sa.pf = a.pf;
-  sa.out_bins = S::M + 1;
-  sa.out_stride = S::M + 1;
-  sa.mag_from_real = 1;
-  sa.out_re = a.out_re + it.out_off;
-  sa.out_im = a.out_im + it.out_off;
-  sa.out_mag = a.out_mag + it.out_off;
-  const StftIO<MODE> io{sa, S::LOGM + 1};
   float2* sm = smem + g * S::SMEM;
-  float2 v[S::R];
-  io.template load<S>(job.y, t, v, sm, tw);
-  fft_engine<S, GroupSync>(v, t, sm, tw);
-  io.template store<S>(job.y, t, v, sm, tw);
+  // a tile holds one or more block-loads of frames (the tuner's tile size),
+  // taken one after the other by the block's groups
+  for (int base = 0; base < tile.y; base += G) {
+    if (base > 0) GroupSync::sync<S>();  // the previous frame's store has read the group's tile
+    const bool ok = base + g < tile.y;
+    const int2 job = __ldg(a.jobs + tile.x + (ok ? base + g : 0));
+    const RaggedItem it = a.items[job.x];
+    StftArgs sa{};
+    sa.pcm = a.pcm + it.pcm_off;
+    sa.pcm_len = it.pcm_len;
+    sa.frames = ok ? (long long)job.y + 1 : 0;  // frame job.y of the item (none when !ok)
+    sa.N = 2 * S::M;
+    sa.W = it.W;
+    sa.H = it.H;
+    sa.win = it.win_off >= 0 ? a.windows + it.win_off : nullptr;
+    sa.pf = a.pf;
+    sa.out_bins = S::M + 1;
+    sa.out_stride = S::M + 1;
+    sa.mag_from_real = 1;
+    sa.out_re = a.out_re + it.out_off;
+    sa.out_im = a.out_im + it.out_off;
+    sa.out_mag = a.out_mag + it.out_off;
+    const StftIO<MODE> io{sa, S::LOGM + 1};
+    float2 v[S::R];
+    io.template load<S>(job.y, t, v, sm, tw);
+    fft_engine<S, GroupSync>(v, t, sm, tw);
+    io.template store<S>(job.y, t, v, sm, tw);
+  }
 }
 
 // ---------------------------------------------------------------- two-half tile

@@ -17,6 +17,7 @@
 #include <cstdlib>
 #include <fstream>
 #include <map>
+#include <random>
 #include <mutex>
 #include <sstream>
 #include <string>
@@ -45,6 +46,7 @@ struct RaggedPlan {
   size_t samples = 0, bins = 0;
   PostFlags pf{};
   int lr[16] = {};                     // pass radix (log2) per log2 N/2 of the single-pass sizes
+  int rounds[16] = {};                 // block-loads of frames per tile per log2 N/2 (0 read as 1)
   int grid = 0, ntiles = 0;
   DevBuf d_items, d_jobs, d_tiles, d_counter, d_scratch, d_windows, d_in, d_re, d_im, d_mag;
   cudaGraph_t graph = nullptr;
@@ -102,7 +104,7 @@ WorkList build_work(const RaggedPlan& p, int only) {
     if (by[L].empty() || (only >= 0 && L != only)) continue;
     const bool whole = ragged_block_log(L) != 0;
     const int T = std::max(1, (1 << L) >> p.lr[L]);
-    const int per = whole ? 1 : std::max(1, ragged_block_threads() / T);
+    const int per = whole ? 1 : std::max(1, ragged_block_threads() / T) * std::max(1, p.rounds[L]);
     for (size_t s = 0; s < by[L].size(); s += per) {
       const int n = (int)std::min<size_t>(per, by[L].size() - s);
       const int lr = (L == ragged_max_log() - 1) ? 0 : p.lr[L];
@@ -140,13 +142,13 @@ RaggedArgs args_for(RaggedPlan& p, const float* pcm, float* re, float* im, float
 }
 
 // ---------------------------------------------------------------- autotuner
-// Cache of measured choices, keyed by (N, frames of that N, transform and
-// kernel generation):
+// Cache of measured choices (pass radix and block-loads of frames per tile),
+// keyed by (N, frames of that N, transform and kernel generation):
 // FFTFREE_TUNE_CACHE names the file (default ~/.cache/fftfree_b200/tune.txt);
 // FFTFREE_TUNE=0 turns tuning off (the default schedule of the size).
-const char* const kTuneKind = "r2c.b1024";  // R2C on the 1024-thread persistent kernel
+const char* const kTuneKind = "r2c.b1024.t";  // R2C on the 1024-thread persistent kernel, radix and tile
 std::mutex g_cache_mu;
-std::map<std::tuple<long long, long long, std::string>, int> g_cache;
+std::map<std::tuple<long long, long long, std::string>, std::pair<int, int>> g_cache;
 bool g_cache_loaded = false;
 
 std::string cache_path() {
@@ -164,14 +166,15 @@ void cache_load() {
     std::istringstream s(line);
     std::string kind, tr;
     long long n = 0, batch = 0;
-    int lr = 0;
-    if (s >> kind >> tr >> n >> batch >> lr && kind == "ragged" && lr >= 2 && lr <= 5)
-      g_cache[{n, batch, tr}] = lr;
+    int lr = 0, rounds = 0;
+    if (s >> kind >> tr >> n >> batch >> lr >> rounds && kind == "ragged" && lr >= 2 && lr <= 5 && rounds >= 1 &&
+        rounds <= 8)
+      g_cache[{n, batch, tr}] = {lr, rounds};
   }
 }
 
-void cache_store(long long n, long long batch, const std::string& tr, int lr) {
-  g_cache[{n, batch, tr}] = lr;
+void cache_store(long long n, long long batch, const std::string& tr, int lr, int rounds) {
+  g_cache[{n, batch, tr}] = {lr, rounds};
   const std::string path = cache_path();
   const size_t slash = path.find_last_of('/');
   if (slash != std::string::npos) {
@@ -181,7 +184,7 @@ void cache_store(long long n, long long batch, const std::string& tr, int lr) {
       if (i == dir.size() || dir[i] == '/') (void)mkdir(dir.substr(0, i).c_str(), 0755);
   }
   std::ofstream f(path, std::ios::app);
-  if (f) f << "ragged " << tr << " " << n << " " << batch << " " << lr << "\n";
+  if (f) f << "ragged " << tr << " " << n << " " << batch << " " << lr << " " << rounds << "\n";
 }
 
 bool tuning_on() {
@@ -209,6 +212,33 @@ float time_launch(RaggedPlan& p, const RaggedArgs& a) {
   return best;
 }
 
+// Per size, largest first: the pass radix among the size's candidates and
+// the tile size (1, 2 or 4 block-loads of frames per claimed tile: more per
+// tile claims fewer tiles, fewer per tile balances the blocks' last tiles
+// better).  Each pair is timed on the whole launch of the plan's work list
+// (the other sizes at their choices so far), since sizes share the
+// persistent blocks; a pair replaces the current choice only when it is at
+// least 0.5% faster.  The samples are uniform in [-1, 1), not the caller's.
+// The tuner's samples: uniform in [-1, 1) (a fixed std::mt19937 draw of up
+// to 2^20 floats, repeated), so that its timings see the arithmetic of real
+// spectra (all-zero frames would take the magnitude's small-value path).
+void fill_tuner_input(RaggedPlan& p) {
+  const size_t n = std::max<size_t>(1, p.samples);
+  float* d = static_cast<float*>(p.d_in.get(n * 4));
+  const size_t m = std::min<size_t>(n, (size_t)1 << 20);
+  std::vector<float> h(m);
+  std::mt19937 gen(7);
+  std::uniform_real_distribution<float> u(-1.0f, 1.0f);
+  for (auto& v : h) v = u(gen);
+  RG_CHECK(cudaMemcpyAsync(d, h.data(), m * 4, cudaMemcpyHostToDevice, p.stream));
+  for (size_t done = m; done < n;) {  // doubling device copies
+    const size_t c = std::min(done, n - done);
+    RG_CHECK(cudaMemcpyAsync(d + done, d, c * 4, cudaMemcpyDeviceToDevice, p.stream));
+    done += c;
+  }
+  RG_CHECK(cudaStreamSynchronize(p.stream));  // the host draw is released on return
+}
+
 void tune(RaggedPlan& p) {
   std::vector<long long> count(ragged_max_log(), 0);
   for (size_t i = 0; i < p.logm.size(); ++i) count[p.logm[i]] += p.frames[i];
@@ -217,33 +247,52 @@ void tune(RaggedPlan& p) {
   for (int L = 0; L < ragged_max_log(); ++L) {
     int cand[4];
     const int nc = ragged_candidates(L, cand);
+    p.rounds[L] = 1;
     if (!count[L] || nc == 0) continue;
     // default: the single-pass kernels' choice for real input, within the candidates
     int def = choose_logr(L, -1, true);
     if (std::find(cand, cand + nc, def) == cand + nc) def = cand[nc - 1];
     p.lr[L] = def;
-    if (nc == 1 || !tuning_on()) continue;
+    // tile sizes worth trying: only while the size has frames for more than
+    // one block-load per tile (whole-block sizes take one frame per tile)
+    std::vector<int> rounds_c{1};
+    if (ragged_block_log(L) == 0) {
+      const long long per = std::max(1, ragged_block_threads() / std::max(1, (1 << L) >> def));
+      for (int r : {2, 4})
+        if (count[L] > per * r) rounds_c.push_back(r);
+    }
+    if ((nc == 1 && rounds_c.size() == 1) || !tuning_on()) continue;
     const long long n = 2LL << L;
     auto it = g_cache.find({n, count[L], kTuneKind});
-    if (it != g_cache.end() && std::find(cand, cand + nc, it->second) != cand + nc) {
-      p.lr[L] = it->second;
+    if (it != g_cache.end() && std::find(cand, cand + nc, it->second.first) != cand + nc) {
+      p.lr[L] = it->second.first;
+      p.rounds[L] = it->second.second;
       continue;
     }
-    float best = 1e30f;
-    int pick = def;
-    for (int c = 0; c < nc; ++c) {
-      p.lr[L] = cand[c];
-      upload(p, build_work(p, L));
+    const auto time_with = [&](int lr, int r) {
+      p.lr[L] = lr;
+      p.rounds[L] = r;
+      upload(p, build_work(p, -1));
       const RaggedArgs a = args_for(p, static_cast<const float*>(p.d_in.p), static_cast<float*>(p.d_re.p),
                                     static_cast<float*>(p.d_im.p), static_cast<float*>(p.d_mag.p));
-      const float ms = time_launch(p, a);
-      if (ms < best) {
-        best = ms;
-        pick = cand[c];
+      return time_launch(p, a);
+    };
+    int pick = def, pick_rounds = 1;
+    float best = time_with(def, 1);
+    for (int c = 0; c < nc; ++c) {
+      for (int r : rounds_c) {
+        if (cand[c] == def && r == 1) continue;
+        const float ms = time_with(cand[c], r);
+        if (ms < 0.995f * best) {
+          best = ms;
+          pick = cand[c];
+          pick_rounds = r;
+        }
       }
     }
     p.lr[L] = pick;
-    cache_store(n, count[L], kTuneKind, pick);
+    p.rounds[L] = pick_rounds;
+    cache_store(n, count[L], kTuneKind, pick, pick_rounds);
   }
 }
 
@@ -364,8 +413,7 @@ FFT_CFFI_API void* fftfree_ragged_plan_stft(const size_t* n, const size_t* lengt
     for (size_t i = 0; i < count; ++i) any_split = any_split || (p->logm[i] == ragged_max_log() - 1 && p->frames[i]);
     if (any_split) p->d_scratch.get((size_t)p->grid * ragged_scratch_per_block());
     // staging (host buffers) and the tuner's buffers
-    RG_CHECK(cudaMemsetAsync(p->d_in.get(std::max<size_t>(1, p->samples) * 4), 0,
-                             std::max<size_t>(1, p->samples) * 4, p->stream));
+    fill_tuner_input(*p);
     p->d_re.get(std::max<size_t>(1, p->bins) * 4);
     p->d_im.get(std::max<size_t>(1, p->bins) * 4);
     p->d_mag.get(std::max<size_t>(1, p->bins) * 4);
@@ -405,6 +453,16 @@ FFT_CFFI_API int fftfree_ragged_schedule(void* plan, size_t n) {
   const int lg = log2_exact(n);
   if (!p || lg < 2 || lg > ragged_max_log()) return 0;
   return (lg - 1 == ragged_max_log() - 1) ? 0 : (1 << p->lr[lg - 1]);
+}
+
+FFT_CFFI_API int fftfree_ragged_tile(void* plan, size_t n) {
+  RaggedPlan* p = as_plan(plan);
+  const int lg = log2_exact(n);
+  if (!p || lg < 2 || lg > ragged_max_log()) return 0;
+  const int L = lg - 1;
+  if (ragged_block_log(L) != 0) return 1;
+  const int T = std::max(1, (1 << L) >> p->lr[L]);
+  return std::max(1, ragged_block_threads() / T) * std::max(1, p->rounds[L]);
 }
 
 FFT_CFFI_API void fftfree_ragged_set_stream(void* plan, void* stream) {

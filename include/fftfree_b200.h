@@ -225,6 +225,10 @@ FFT_CFFI_API size_t fftfree_ragged_bins(void* plan);
 /* The pass radix the plan runs for size n (0: n is absent from the plan's
  * single-pass sizes, or takes the two-half path of 65536 points). */
 FFT_CFFI_API int fftfree_ragged_schedule(void* plan, size_t n);
+/* Frames of size n per tile that a block of the plan's launch claims at once
+ * (one or more block-loads, the tuner's tile size; 1 for the sizes that take
+ * a whole block per frame, 0 for a NULL plan or an unsupported n). */
+FFT_CFFI_API int fftfree_ragged_tile(void* plan, size_t n);
 /* Stream of the plan's launches (NULL: the plan's own stream). */
 FFT_CFFI_API void fftfree_ragged_set_stream(void* plan, void* cuda_stream);
 /* Runs the plan: host or device buffers (host ones are staged and the call

@@ -138,6 +138,40 @@ def test_ragged_host_buffers_and_graph_reuse(monkeypatch, tmp_path):
     np.testing.assert_array_equal(run_plan(plan2, pcm)[2], first[2])
 
 
+def test_ragged_tuner_tile_sizes(monkeypatch, tmp_path):
+    """The tuner's tile size (block-loads of frames per claimed tile): a
+    workload with many frames of a few small sizes lets it try tiles of 1, 2
+    and 4 block-loads; whatever it picks is a whole number of block-loads,
+    it is cached beside the radix, and the outputs are the same bits as the
+    tuner-off plan's wherever the radix is the same (the tile only changes
+    which block takes which frames)."""
+    cache = tmp_path / "tune.txt"
+    monkeypatch.setenv("FFTFREE_TUNE_CACHE", str(cache))
+    rng = np.random.default_rng(21)
+    sizes = [int(v) for v in rng.choice([64, 256, 1024, 2048], 6000)]
+    pcm = np.concatenate([rng.uniform(-1, 1, n).astype(np.float32) for n in sizes])
+    plan = api.RaggedPlan(sizes)
+    got = run_plan(plan, pcm)
+    lines = [ln.split() for ln in cache.read_text().splitlines()]
+    assert lines and all(len(ln) == 6 and ln[0] == "ragged" for ln in lines)
+    monkeypatch.setenv("FFTFREE_TUNE", "0")
+    base = api.RaggedPlan(sizes)
+    ref = run_plan(base, pcm)
+    for n in set(sizes):
+        T = max(1, (n // 2) // plan.schedule(n))
+        per = max(1, 1024 // T)
+        assert plan.tile(n) in (per, 2 * per, 4 * per), (n, plan.tile(n), per)
+        assert base.tile(n) == max(1, 1024 // max(1, (n // 2) // base.schedule(n)))
+    off = 0
+    for n in sizes:
+        b = n // 2 + 1
+        if plan.schedule(n) == base.schedule(n):
+            for g, r in zip(got, ref):
+                np.testing.assert_array_equal(g[off: off + b], r[off: off + b])
+        off += b
+    assert plan.tile(65536) == 1 and plan.tile(3) == 0
+
+
 def test_ragged_small_sizes_and_rejects():
     sizes = [4, 8, 16, 32, 64, 4, 128, 65536, 8]
     rng = np.random.default_rng(9)
