@@ -11,13 +11,18 @@
 // transform.  dL/dx[t] = sum over the frames f covering t of
 // w[t - f*H] * dL/ds_f[t - f*H].
 //
-// The spectrum is recomputed from x rather than stored by the forward
-// pass.  Each block owns `span` consecutive samples of one signal and
-// transforms every frame that touches them (a few frames of halo per block
-// are transformed by both neighbours); the overlap-add adjoint is a gather
-// in frame order through a shared-memory accumulator, so the result is
-// deterministic and needs no atomics.
+// The spectrum comes from the unit phasor X / |X| the forward pass saved, or
+// is recomputed from x (long signals).  Two forms of the overlap-add
+// adjoint, both gathers in frame order (deterministic, no atomics): the
+// sliding form (hops N / 2^q) walks a run of frames per thread group and
+// sums in a register window; the general form gives each block `span`
+// consecutive samples of one signal, transforms every frame that touches
+// them (a few frames of halo per block are transformed by both neighbours)
+// and sums through a shared-memory accumulator.
 #include <cstdlib>
+#include <map>
+#include <mutex>
+#include <utility>
 
 #include "fft_launch.cuh"
 
@@ -479,14 +484,31 @@ static int slide_logr(int logm) {
 // leave 40 SMs with one block instead of two.
 static long long slide_run(const MagGradArgs& a, const void* fn, int block, size_t smem, int G, int halo) {
   if (a.run > 0) return a.run;
-  int dev = 0, sms = 0, per_sm = 0;
-  if (cudaGetDevice(&dev) != cudaSuccess || cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) !=
-      cudaSuccess || cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, block, smem) != cudaSuccess ||
-      per_sm < 1) {
+  // resident blocks of this kernel on this device, queried once
+  static std::mutex mu;
+  static std::map<std::pair<const void*, int>, long long> resident;
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) {
     cudaGetLastError();
     return 32;
   }
-  const long long slots = (long long)sms * per_sm * G;
+  long long blocks = 0;
+  {
+    std::lock_guard<std::mutex> lk(mu);
+    auto it = resident.find({fn, dev});
+    if (it != resident.end()) {
+      blocks = it->second;
+    } else {
+      int sms = 0, per_sm = 0;
+      if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess ||
+          cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, block, smem) != cudaSuccess || per_sm < 1) {
+        cudaGetLastError();
+        return 32;
+      }
+      blocks = resident[{fn, dev}] = (long long)sms * per_sm;
+    }
+  }
+  const long long slots = blocks * G;
   long long best = 32, best_cost = -1;
   for (long long run = 16; run <= 64; ++run) {
     const long long jobs = a.signals * ((a.frames + run - 1) / run);
