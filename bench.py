@@ -494,9 +494,11 @@ def main():
     kern_avg = sum(kern_ms) / len(kern_ms)
     achieved = BYTES_PER_PASS / (kern_avg * 1e-3) / 1e9
 
-    # secondary legs on the same device (information; not the headline)
+    # secondary legs on the same device (information; not the headline).  One
+    # GPU only: under torchrun the other ranks would wait for rank 0's legs
+    # in the next collective.
     legs = {}
-    if rank == 0 and not args.no_legs:
+    if rank == 0 and world == 1 and not args.no_legs:
         legs = measure_legs(ff, torch, stream)
 
     # e2e through the C ABI with pinned host buffers
