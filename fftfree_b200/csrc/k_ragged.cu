@@ -145,15 +145,18 @@ __device__ __forceinline__ void ragged_split(const RaggedArgs& a, int4 tile, flo
   float* im = a.out_im + it.out_off + (long long)job.y * (M + 1);
   float* mg = a.out_mag + it.out_off + (long long)job.y * (M + 1);
   // w_M^k and w_N^k for k = t + i T: w^t (one pyramid load per thread) times
-  // a compile-time constant (M / T = 32 and N / T = 64), rounded term by term
-  // -- the large pyramid levels (256 and 512 KB) are not read per bin
-  static_assert(M / T == 2 * R && 2 * M / T == 4 * R, "combine twiddles from constants");
+  // w_32^i and w_64^i (M / T = 32, N / T = 64), rounded term by term, the
+  // latter read from the pyramid's small levels 5 and 6 (the same entry for
+  // the whole warp); the large levels (256 and 512 KB) are not read per bin,
+  // and the loop stays rolled (the kernel's code already strains the
+  // instruction cache)
+  static_assert(M / T == 32 && 2 * M / T == 64, "combine twiddles from levels 5 and 6");
   const float2 wMt = tw_get(tw, LM, (unsigned)t);
   const float2 wNt = tw_get(tw, LM + 1, (unsigned)t);
-#pragma unroll
+#pragma unroll 2
   for (int i = 0; i < R; ++i) {
     const int k = t + i * T;
-    const float2 wk = i == 0 ? wMt : cmul_rn(wMt, wconst<2 * R>(i));  // w_M^k
+    const float2 wk = i == 0 ? wMt : cmul_rn(wMt, tw_get(tw, 5, (unsigned)i));  // w_M^k
     const float2 e = scr[k];
     const float2 o = cmul(smem[pidx(k)], wk);  // O[k] (from the tile: the registers go to the combine)
     const float2 zk = cadd(e, o);                       // Z[k]
@@ -169,7 +172,7 @@ __device__ __forceinline__ void ragged_split(const RaggedArgs& a, int4 tile, flo
       zmk2 = cadd(em, om);
       zmk = csub(em, om);
     }
-    const float2 wn = i == 0 ? wNt : cmul_rn(wNt, wconst<4 * R>(i));  // w_N^k
+    const float2 wn = i == 0 ? wNt : cmul_rn(wNt, tw_get(tw, 6, (unsigned)i));  // w_N^k
     const float2 h = make_float2(0.5f * wn.x, 0.5f * wn.y);
     const float2 h2 = make_float2(0.5f * wn.y, -0.5f * wn.x);  // w_N^(k + M/2) / 2 = -i w_N^k / 2
     float2 X = untangle_bin(zk, zmk, h);
