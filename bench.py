@@ -206,23 +206,27 @@ def _cpu_reference_run(steps: int, warmup: int, budget_s: float = None):
     return dt, threads, kind, sample
 
 
-def _in_child(func: str, attempts: int = 3, **kw):
+def _in_child(func: str, attempts: int = 3, timeout_s: float = 180.0, **kw):
     """Runs bench.<func>(**kw) in a fresh Python process (no CUDA context) and
-    returns its JSON-able result, or None when every attempt died.  The
-    reference's WorkerPool has crashed intermittently on the GPU box's 16
-    host threads (a segfault or abort in its own code, during or after a
-    call); in a child process such a crash costs one attempt, not the bench."""
+    returns its JSON-able result, or None when every attempt died or ran past
+    timeout_s.  The reference's WorkerPool has crashed intermittently on the
+    GPU box's 16 host threads (a segfault or abort in its own code, during or
+    after a call); in a child process such a crash costs one attempt, not the
+    bench.  The end of a failed attempt's stderr goes to this stderr."""
     code = ("import json, sys; sys.path.insert(0, %r); import bench; "
             "print('@@RESULT ' + json.dumps(bench.%s(**json.loads(sys.argv[1]))), flush=True)" % (REPO, func))
-    for _ in range(attempts):
+    for attempt in range(attempts):
         try:
             r = subprocess.run([sys.executable, "-c", code, json.dumps(kw)], capture_output=True, text=True,
-                               timeout=900)
+                               timeout=timeout_s)
         except subprocess.TimeoutExpired:
+            sys.stderr.write(f"[bench] {func}: attempt {attempt + 1} ran past {timeout_s:.0f} s\n")
             continue
         for line in r.stdout.splitlines():
             if line.startswith("@@RESULT "):
                 return json.loads(line[len("@@RESULT "):])
+        sys.stderr.write(f"[bench] {func}: attempt {attempt + 1} exited {r.returncode}: "
+                         f"{r.stderr.strip()[-300:]}\n")
     return None
 
 
@@ -234,7 +238,7 @@ def _cpu_reference_child(steps: int, warmup: int, budget_s: float = None):
 def cpu_baseline(budget_s: float = 15.0):
     """The reference's CPU path on the host cores (bounded: about budget_s),
     in a child process."""
-    r = _in_child("_cpu_reference_child", steps=1000, warmup=1, budget_s=budget_s)
+    r = _in_child("_cpu_reference_child", timeout_s=budget_s + 120.0, steps=1000, warmup=1, budget_s=budget_s)
     if r is None:
         return {"unavailable": "the reference's CPU run crashed in every attempt (its WorkerPool)"}
     return {"value": round(BYTES_PER_PASS / r["dt"] / 1e9, 3), "unit": "GB/s", "cores": r["threads"],
@@ -244,7 +248,9 @@ def cpu_baseline(budget_s: float = 15.0):
 def run_reference(args, rank, world):
     if rank != 0:
         return 0
-    r = _in_child("_cpu_reference_child", steps=args.steps, warmup=args.warmup)
+    # a step is about 0.1 s of the reference on 16 threads: generous room
+    r = _in_child("_cpu_reference_child", timeout_s=120.0 + 5.0 * (args.steps + args.warmup), steps=args.steps,
+                  warmup=args.warmup)
     if r is None:
         print(json.dumps({"impl": "reference", "unavailable": "the reference's CPU run crashed in every attempt "
                                                               "(a segfault in its own WorkerPool)"}), flush=True)
@@ -710,7 +716,7 @@ def measure_griffin_lim(ff, torch, reps: int = 5):
            "setup_ms": round(ms32 - 32 * (ms96 - ms32) / 64, 3)}
     fc.close()
     ic.close()
-    ref = _in_child("_ref_griffin_lim", N=N, H=H, F=F)
+    ref = _in_child("_ref_griffin_lim", timeout_s=120.0, N=N, H=H, F=F)
     leg["cpu_baseline"] = ref if ref is not None else {
         "unavailable": "the reference's fft_griffin_lim crashed in every attempt (its WorkerPool)"}
     return leg
