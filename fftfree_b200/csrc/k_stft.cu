@@ -12,8 +12,8 @@ namespace {
 // samples, which one thread copies into shared memory with one bulk copy
 // (cp.async.bulk, completion counted on an mbarrier), with the analysis
 // window beside it; the groups then frame from shared memory instead of
-// re-reading each sample N / H times through L1.  No multicast; the source
-// is this GPU's own buffer.  A block whose frames do not all lie inside the
+// re-reading each sample N / H times through L1.  Each block copies for
+// itself only, from this GPU's own buffer.  A block whose frames do not all lie inside the
 // signal, or whose bounded wait for the copy gives up, loads from global
 // memory as the other kernels do (the copy is then drained, bounded, before
 // the block exits).

@@ -25,7 +25,7 @@
 // Operands live in shared memory in the no-swizzle K-major layout of the MMA
 // descriptors: 8-row x 16-byte core matrices, the two of one K = 16 step
 // 128 B apart (leading byte offset), consecutive 8-row groups 512 B apart
-// (stride byte offset).  Single-GPU code: no cluster, no multicast.
+// (stride byte offset).  Single-GPU code: no cluster; every copy is one CTA's own.
 #include <cuda_fp16.h>
 
 #include <cstdlib>
