@@ -8,8 +8,10 @@
 // Pass B: row FFTs of length N2 for C consecutive rows per block; results are
 //   staged through shared memory so that the writes of X[k1 + N1 k2] walk
 //   consecutive k1.
-// The batch runs in chunks whose scratch (chunk * N complex) stays resident
-// in the 126 MB L2, so pass B reads pass A's output from L2, not HBM.
+// The batch runs in chunks of scratch (chunk * N complex, up to 1 GiB by
+// default: one chunk for most batches, both passes then streaming through
+// HBM); with several chunks, pass A of the next chunk overlaps pass B of
+// the current one on a second stream.
 // Each IO policy supplies elem4 (input element n) and emit4 (output bin k)
 // with the same hook semantics as the single-pass kernels.
 #include <algorithm>

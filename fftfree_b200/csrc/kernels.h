@@ -236,8 +236,8 @@ int ragged_block_threads();           // threads per block of the persistent ker
 cudaError_t launch_ragged(const RaggedArgs& a, int grid, cudaStream_t s, uint64_t* launches);
 
 // Multi-pass (four-step) transforms for 2^14 <= N <= 2^20.  `scratch` holds
-// `chunk` transforms of N complex points (four_step_chunk picks a chunk
-// that stays resident in L2).
+// `chunk` transforms of N complex points (four_step_chunk picks the chunk:
+// up to 1 GiB of scratch by default).
 int max_multi_pass_log();
 size_t four_step_chunk(int log_n, long long batch);
 cudaError_t launch_four_step_stft(const StftArgs& a, float2* scratch, size_t chunk, cudaStream_t s,
