@@ -52,9 +52,9 @@ struct StftArgs {
 long long stft_loss_parts(long long frames, int N);
 
 // Gradient of the magnitude STFT (forward R2C half spectrum, |X| per bin)
-// with respect to the signals: recomputes each frame's spectrum, applies
-// the magnitude chain rule, the adjoint transform and the windowed
-// overlap-add adjoint of framing.
+// with respect to the signals: each frame's spectrum from the saved unit
+// phasor or recomputed from the signal, the magnitude chain rule, the
+// adjoint transform and the windowed overlap-add adjoint of framing.
 struct MagGradArgs {
   const float* pcm;       // signals x sig_stride, each pcm_len samples
   long long signals;
@@ -149,8 +149,6 @@ cudaError_t launch_transpose(const float2* in, float2* out, long long rows, long
                              cudaStream_t s, uint64_t* launches);
 cudaError_t launch_cplx_batch(const CplxBatchArgs& a, int logr, cudaStream_t s, uint64_t* launches);
 cudaError_t launch_ola(const OlaArgs& a, cudaStream_t s, uint64_t* launches);
-// Griffin-Lim projection: re + i im = mag e^{i atan2(ti, tr)} (half spectrum:
-// DC and, for even N, Nyquist imaginary parts cleared).
 // 256-point C2C transforms (no hooks) on the tcgen05 tensor cores in split
 // FP16 (k_tc05.cu), chosen when FFTFREE_TC16=2; the count of blocks whose
 // bounded wait on an MMA commit gave up (their outputs are left unwritten).
@@ -161,6 +159,8 @@ unsigned tc05_timeouts();
 // Griffin-Lim initial spectra: re = mag * cs.x, im = mag * cs.y (cs: the
 // cosines and sines of the initial phases).
 cudaError_t launch_gl_init(const float* mag, const float2* cs, float* re, float* im, long long n, cudaStream_t s);
+// Griffin-Lim projection: re + i im = mag e^{i atan2(ti, tr)} (half spectrum:
+// DC and, for even N, Nyquist imaginary parts cleared).
 cudaError_t launch_gl_project(const float* mag, const float* tr, const float* ti, float* re, float* im,
                               long long nbins, int bins, int half, int even_n, cudaStream_t s);
 // Streaming ISTFT step (fft_cffi.cpp:1597-1742): F inverse frames of N
