@@ -22,6 +22,7 @@
 #include <cstdlib>
 #include <map>
 #include <mutex>
+#include <tuple>
 #include <utility>
 
 #include "fft_launch.cuh"
@@ -355,7 +356,8 @@ __device__ __forceinline__ void store_pair(float* out, long long p, long long L,
 
 // One frame into the register window at rotation ROT: slot i of the frame
 // (samples 2(t + iT) + {0, 1} past its start) adds into acc[(i + ROT*SH) % R]
-// as one FFMA2 with the window taps; v holds (dL/ds[2m], -dL/ds[2m+1]), so
+// as one FFMA2 with the window taps (w2: the block's copy in shared memory,
+// or null for no window); v holds (dL/ds[2m], -dL/ds[2m+1]), so
 // the window keeps the second sum negated.  The SH slots that are then
 // complete (acc[ROT*SH ..]) are written when `store` and cleared for the
 // frames to come.  Rotating the window instead of shifting it costs no
@@ -366,7 +368,7 @@ __device__ __forceinline__ void slide_step(float2 (&acc)[S::R], const float2 (&v
   constexpr int T = S::T, R = S::R, SH = R >> QL;
 #pragma unroll
   for (int i = 0; i < R; ++i) {
-    const float2 w = w2 ? __ldg(w2 + t + i * T) : make_float2(1.f, 1.f);
+    const float2 w = w2 ? w2[t + i * T] : make_float2(1.f, 1.f);  // w2: shared memory
     acc[(i + ROT * SH) % R] = __ffma2_rn(v[i], w, acc[(i + ROT * SH) % R]);
   }
   if (store) {
@@ -415,6 +417,15 @@ __global__ void __launch_bounds__(Launch<S>::BLOCK, slide_min_blocks<S>()) k_stf
   const int g = threadIdx.x / T;
   const int t = threadIdx.x - g * T;
   float2* sm = smem + g * S::SMEM;
+  // the window taps, once per block in shared memory after the groups' tiles
+  // (every group reads the same taps at the same slots for every frame)
+  const float2* w2 = nullptr;
+  if (a.win) {
+    float* wsm = reinterpret_cast<float*>(smem + G * S::SMEM);
+    for (int p = threadIdx.x; p < 2 * M; p += blockDim.x) wsm[p] = __ldg(a.win + p);
+    __syncthreads();
+    w2 = reinterpret_cast<const float2*>(wsm);
+  }
   const long long runs = (a.frames + a.run - 1) / a.run;
   const long long job = (long long)blockIdx.x * G + g;
   if (job >= a.signals * runs) return;  // the whole group leaves; no block barrier follows
@@ -429,7 +440,6 @@ __global__ void __launch_bounds__(Launch<S>::BLOCK, slide_min_blocks<S>()) k_stf
   float* out = a.grad_pcm + sig * a.sig_stride;
   const long long L = a.pcm_len;
   const bool vec = aligned8(out);
-  const float2* w2 = reinterpret_cast<const float2*>(a.win);  // 8-byte aligned (checked by the launcher)
 
   float2 acc[R];
 #pragma unroll
@@ -486,7 +496,7 @@ static long long slide_run(const MagGradArgs& a, const void* fn, int block, size
   if (a.run > 0) return a.run;
   // resident blocks of this kernel on this device, queried once
   static std::mutex mu;
-  static std::map<std::pair<const void*, int>, long long> resident;
+  static std::map<std::tuple<const void*, int, size_t>, long long> resident;
   int dev = 0;
   if (cudaGetDevice(&dev) != cudaSuccess) {
     cudaGetLastError();
@@ -495,7 +505,7 @@ static long long slide_run(const MagGradArgs& a, const void* fn, int block, size
   long long blocks = 0;
   {
     std::lock_guard<std::mutex> lk(mu);
-    auto it = resident.find({fn, dev});
+    auto it = resident.find({fn, dev, smem});
     if (it != resident.end()) {
       blocks = it->second;
     } else {
@@ -505,7 +515,7 @@ static long long slide_run(const MagGradArgs& a, const void* fn, int block, size
         cudaGetLastError();
         return 32;
       }
-      blocks = resident[{fn, dev}] = (long long)sms * per_sm;
+      blocks = resident[{fn, dev, smem}] = (long long)sms * per_sm;
     }
   }
   const long long slots = blocks * G;
@@ -521,7 +531,8 @@ static long long slide_run(const MagGradArgs& a, const void* fn, int block, size
 template <class S, int QL, bool PH>
 static cudaError_t launch_slide(const MagGradArgs& a0, cudaStream_t st, uint64_t* launches) {
   using L = Launch<S>;
-  const size_t smem = (size_t)L::G * S::SMEM * sizeof(float2);
+  // the groups' tiles, then the window taps
+  const size_t smem = (size_t)L::G * S::SMEM * sizeof(float2) + (a0.win ? (size_t)a0.N * sizeof(float) : 0);
   if (smem > 48 * 1024) {
     const cudaError_t e = cudaFuncSetAttribute(k_stft_mag_grad_slide<S, QL, PH>,
                                                cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
